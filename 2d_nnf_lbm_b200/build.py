@@ -1,0 +1,80 @@
+"""Build liblbm2d.so (the CUDA library behind include/lbm2d.h) in-tree.
+
+Every translation unit is compiled for sm_100a only.  The FP64 lattice
+kernel and the particle kernel are built with --fmad=false so that their
+arithmetic follows the reference operation by operation; the FP32 kernel
+keeps fused multiply-adds.
+
+    python -m 2d_nnf_lbm_b200.build        (or build() from Python)
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "liblbm2d.so")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
+          "--expt-relaxed-constexpr"]
+
+SOURCES = {
+    "lbm_fp64.cu": ["--fmad=false"],
+    "lbm_fp32.cu": ["--fmad=true"],
+    "lbm_particles.cu": ["--fmad=false"],
+    "lbm_api.cu": [],
+}
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(HERE, "..", "include", "lbm2d.h"))
+    objs = []
+    logs = []
+    for src, extra in SOURCES.items():
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _stale(o, [s, *headers, __file__]):
+            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", s, "-o", o]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            logs.append(r.stdout + r.stderr)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError(f"nvcc failed on {src}")
+    if force or _stale(OUT, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("link failed")
+    with open(os.path.join(BUILD_DIR, "ptxas.log"), "a") as fh:
+        fh.write("".join(logs))
+    if verbose:
+        print("".join(logs))
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,849 @@
+// lbm_api.cu -- C ABI of include/lbm2d.h: handle life cycle, the per-step
+// launch sequence, and the getters/setters.
+//
+// Per time step the host enqueues two kernels on the handle's stream:
+//   k_particles  repulsion, Newton-Euler update, history, tile lists
+//   k_lattice    stream + BC + macro + SPM + force partials + correction +
+//                collision of the next step (last block reduces FORCE)
+// The post-collision populations live in a ping-pong pair: after step K,
+// f[cur] holds f*(K+1) and f[cur^1] holds f*(K), from which the output
+// kernel re-derives the fields of step K (F after BC, rho, u, G, PHI) on
+// demand without touching the state.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm2d.h"
+#include "lbm_internal.h"
+
+using namespace lbm;
+
+struct lbm_sim {
+  lbm_params p;
+  cudaStream_t stream = nullptr;
+  Geometry g{};
+  Model m{};
+  int prec = 0;
+  size_t esz = 8;
+  void* f[2] = {nullptr, nullptr};
+  void* om[2] = {nullptr, nullptr};
+  void* rec = nullptr;
+  int cur = 0;
+  bool prev_post_bc = false;
+  int64_t kk = 0;
+  // particles
+  int np = 0;
+  int np_cap = 0;
+  double* ps = nullptr;
+  int4* tbox = nullptr;
+  int* tile_count = nullptr;
+  int* tile_list = nullptr;
+  int tile_cap = MAX_TILE_CAND;
+  int max_slots = 1;
+  double* partials = nullptr;
+  int* cell_count = nullptr;
+  int* cell_start = nullptr;
+  int* cell_items = nullptr;
+  int* cell_of = nullptr;
+  int ncx = 1, ncy = 1;
+  double cell_size = 1.0;
+  // scalars
+  unsigned int* ticket = nullptr;
+  double* mass_partials = nullptr;
+  long long* d_kk = nullptr;
+  double* stale_dpw = nullptr;
+  int* h_status = nullptr;  // pinned copy of d_status, refreshed after each call
+  int* d_status = nullptr;  // sticky ST_* bits written by the kernels
+  // history
+  double* series = nullptr;
+  int series_len = LBM_SERIES_HEAD;
+  int series_cap = 0;
+  int series_np = 0;
+  int64_t drained_kk = 0;
+  std::vector<double> host_series;
+  size_t host_series_read = 0;
+  // output scratch
+  double* out = nullptr;
+  double* out_f = nullptr;
+  int64_t out_kk = -1;
+};
+
+namespace {
+
+constexpr int NOUT = 7;  // ux uy rho phi gx gy pnode
+
+int cuda_fail(cudaError_t e) {
+  if (e == cudaErrorMemoryAllocation) return LBM_E_NOMEM;
+  return LBM_E_CUDA;
+}
+
+#define CK(expr)                                 \
+  do {                                           \
+    cudaError_t e_ = (expr);                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_); \
+  } while (0)
+
+template <class T>
+int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(e);
+  }
+  return LBM_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+// All copies are ordered on the handle's (non-blocking) stream; copies to the
+// host wait for completion.
+cudaError_t h2d(lbm_sim* h, void* dst, const void* src, size_t bytes) {
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+}
+cudaError_t d2h(lbm_sim* h, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(h->stream);
+}
+
+long long nodes(const lbm_sim* h) { return (long long)(h->p.nx + 1) * (h->p.ny + 1); }
+
+int sticky_status(const lbm_sim* h) {
+  const int s = *(volatile int*)h->h_status;  // as of the last completed copy
+  if (s & ST_NAN) return LBM_E_NAN;
+  if (s & ST_OVERFLOW) return LBM_E_OVERFLOW;
+  if (s & ST_TIMEOUT) return LBM_E_TIMEOUT;
+  if (s & ST_PARTICLE) return LBM_E_PARTICLE;
+  return LBM_OK;
+}
+
+// Synchronising variant for the getters.
+int refreshed_status(lbm_sim* h) {
+  if (cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return LBM_E_CUDA;
+  return sticky_status(h);
+}
+
+LatticeArgs lattice_args(lbm_sim* h) {
+  LatticeArgs a{};
+  a.g = h->g;
+  a.m = h->m;
+  a.src = h->f[h->cur];
+  a.dst = h->f[h->cur ^ 1];
+  a.om_src = h->om[h->cur];
+  a.om_dst = h->om[h->cur ^ 1];
+  a.ps = h->ps;
+  a.ps_force = h->ps;
+  a.np = h->np;
+  a.tile_count = h->tile_count;
+  a.tile_list = h->tile_list;
+  a.tile_cap = h->tile_cap;
+  a.tbox = h->tbox;
+  a.partials = h->partials;
+  a.max_slots = h->max_slots;
+  a.ticket = h->ticket;
+  a.mass_partials = h->mass_partials;
+  a.kk = h->d_kk;
+  a.series = h->series;
+  a.series_every = h->p.series_every;
+  a.series_cap = h->series_cap;
+  a.series_len = h->series_len;
+  a.status = h->d_status;
+  a.rec = h->rec;
+  return a;
+}
+
+ParticleArgs particle_args(lbm_sim* h) {
+  ParticleArgs a{};
+  a.ps = h->ps;
+  a.np = h->np;
+  a.tbox = h->tbox;
+  a.tile_count = h->tile_count;
+  a.tile_list = h->tile_list;
+  a.tile_cap = h->tile_cap;
+  a.max_slots = h->max_slots;
+  a.wall_model = h->p.wall_model;
+  a.contact = h->p.contact_test;
+  a.rep_zeta = h->p.rep_zeta;
+  a.eps_p = h->p.eps_p;
+  a.eps_w = h->p.eps_w;
+  a.e_p = h->p.e_p;
+  a.e_w = h->p.e_w;
+  a.c_ij = h->p.c_ij;
+  a.mirror_top = h->p.wall_mirror_top;
+  a.mirror_left = h->p.wall_mirror_left;
+  a.rho0 = h->p.rho0;
+  a.gravity = h->p.gravity;
+  a.integrate_angle = h->p.integrate_angle;
+  a.cell_count = h->cell_count;
+  a.cell_start = h->cell_start;
+  a.cell_items = h->cell_items;
+  a.cell_of = h->cell_of;
+  a.ncx = h->ncx;
+  a.ncy = h->ncy;
+  a.cell_size = h->cell_size;
+  a.stale_dpw = h->stale_dpw;
+  a.kk = h->d_kk;
+  a.series = h->series;
+  a.series_every = h->p.series_every;
+  a.series_cap = h->series_cap;
+  a.series_len = h->series_len;
+  a.series_np = h->series_np;
+  a.status = h->d_status;
+  a.nx = h->p.nx;
+  a.ny = h->p.ny;
+  a.zeta = h->p.zeta;
+  return a;
+}
+
+cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
+  if (h->prec == LBM_FP64) {
+    switch (mode) {
+      case 0: return launch_step_fp64(a, h->stream);
+      case 1: return launch_output_fp64(a, h->stream);
+      case 2: return launch_init_fp64(a, h->stream);
+      default: return launch_restart_fp64(a, h->stream);
+    }
+  }
+  switch (mode) {
+    case 0: return launch_step_fp32(a, h->stream);
+    case 1: return launch_output_fp32(a, h->stream);
+    case 2: return launch_init_fp32(a, h->stream);
+    default: return launch_restart_fp32(a, h->stream);
+  }
+}
+
+// Copy history records of steps (drained_kk, kk] from the device ring.
+int drain_series(lbm_sim* h) {
+  const int every = h->p.series_every;
+  if (!h->series || every <= 0) {
+    h->drained_kk = h->kk;
+    return LBM_OK;
+  }
+  long long r0 = h->drained_kk / every, r1 = h->kk / every;  // records r0..r1-1
+  if (r1 <= r0) {
+    h->drained_kk = h->kk;
+    return LBM_OK;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t len = (size_t)h->series_len;
+  const size_t old = h->host_series.size();
+  h->host_series.resize(old + (size_t)(r1 - r0) * len);
+  double* dst = h->host_series.data() + old;
+  long long r = r0;
+  while (r < r1) {
+    const long long slot = r % h->series_cap;
+    long long cnt = std::min<long long>(r1 - r, h->series_cap - slot);
+    CK(d2h(h, dst, h->series + slot * len, (size_t)cnt * len * sizeof(double)));
+    dst += cnt * len;
+    r += cnt;
+  }
+  h->drained_kk = h->kk;
+  return LBM_OK;
+}
+
+// Fields of step kk in h->out (and F after BC in h->out_f when want_f).
+int compute_output(lbm_sim* h, bool want_f) {
+  if (h->out_kk == h->kk && (!want_f || h->out_f)) return LBM_OK;
+  LatticeArgs a = lattice_args(h);
+  a.src = h->f[h->cur ^ 1];
+  a.om_src = h->om[h->cur ^ 1];
+  a.out = h->out;
+  a.out_f = want_f ? h->out_f : nullptr;
+  a.src_post_bc = h->prev_post_bc ? 1 : 0;
+  a.initial = (h->kk == 0 && !h->prev_post_bc) ? 1 : 0;
+  CK(launch_lattice(h, a, 1));
+  CK(cudaStreamSynchronize(h->stream));
+  h->out_kk = h->kk;
+  return LBM_OK;
+}
+
+int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
+  // free old
+  dfree(h->ps); dfree(h->tbox); dfree(h->partials);
+  dfree(h->cell_count); dfree(h->cell_start); dfree(h->cell_items); dfree(h->cell_of);
+  dfree(h->series);
+  h->ps = nullptr; h->tbox = nullptr; h->partials = nullptr;
+  h->cell_count = h->cell_start = h->cell_items = h->cell_of = nullptr;
+  h->series = nullptr;
+  h->np = np;
+  // tile boxes: radius R + zeta/2 + 1 around the centre
+  const double r = 0.5 * dmax + 0.5 * h->p.zeta + 1.0;
+  const int mtx = (int)std::floor(2.0 * r / TX) + 2;
+  const int mty = (int)std::floor(2.0 * r / TY) + 2;
+  h->max_slots = std::max(1, std::min(mtx, h->g.nbx) * std::min(mty, h->g.nby));
+  h->cell_size = std::max(1.0, dmax + h->p.rep_zeta) * (1.0 + 1e-9);
+  h->ncx = std::max(1, (int)std::floor((double)h->p.nx / h->cell_size) + 1);
+  h->ncy = std::max(1, (int)std::floor((double)h->p.ny / h->cell_size) + 1);
+  int rc;
+  if ((rc = dalloc(&h->ps, (size_t)std::max(np, 1) * PS))) return rc;
+  if ((rc = dalloc(&h->tbox, (size_t)std::max(np, 1)))) return rc;
+  if ((rc = dalloc(&h->partials, (size_t)std::max(np, 1) * h->max_slots * 3))) return rc;
+  const size_t ncells = (size_t)h->ncx * h->ncy;
+  if ((rc = dalloc(&h->cell_count, ncells + 1))) return rc;
+  if ((rc = dalloc(&h->cell_start, ncells + 1))) return rc;
+  if ((rc = dalloc(&h->cell_items, (size_t)std::max(np, 1)))) return rc;
+  if ((rc = dalloc(&h->cell_of, (size_t)std::max(np, 1)))) return rc;
+  CK(cudaMemsetAsync(h->tbox, 0, sizeof(int4) * std::max(np, 1), h->stream));
+  CK(cudaMemsetAsync(h->partials, 0, sizeof(double) * std::max(np, 1) * h->max_slots * 3,
+                     h->stream));
+  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * h->g.nbx * h->g.nby, h->stream));
+  h->series_np = std::max(0, std::min(h->p.series_particles, np));
+  h->series_len = LBM_SERIES_HEAD + LBM_SERIES_PER * h->series_np;
+  h->series_cap = std::max(1, h->p.series_capacity);
+  if (h->p.series_every > 0) {
+    if ((rc = dalloc(&h->series, (size_t)h->series_cap * h->series_len))) return rc;
+  }
+  return LBM_OK;
+}
+
+void particle_record(const lbm_params& p, double* P, double x, double y, double ang, double u,
+                     double v, double w, double diam, double rho_p) {
+  std::memset(P, 0, sizeof(double) * PS);
+  P[P_X] = x;
+  P[P_Y] = y;
+  P[P_ANG] = ang;
+  P[P_U] = u;
+  P[P_V] = v;
+  P[P_W] = w;
+  P[P_D] = diam;
+  P[P_RHO] = rho_p;
+  // M_P and I_P as C1:178-179
+  P[P_M] = rho_p * p.pi * (0.5 * diam) * (0.5 * diam);
+  P[P_I] = 0.5 * P[P_M] * (0.5 * diam) * (0.5 * diam);
+}
+
+int launch_tiles(lbm_sim* h) {
+  ParticleArgs pa = particle_args(h);
+  CK(launch_tiles_only(pa, h->stream));
+  return LBM_OK;
+}
+
+template <class T>
+void to_pitched(const double* src_dense, std::vector<unsigned char>& buf, const lbm_sim* h,
+                int planes, bool aos9, bool shift) {
+  const int n1x = h->p.nx + 1, n1y = h->p.ny + 1;
+  buf.assign((size_t)planes * h->g.plane * sizeof(T), 0);
+  T* d = reinterpret_cast<T*>(buf.data());
+  static const double w[9] = {4.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9,
+                              1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
+  for (int k = 0; k < planes; ++k)
+    for (int j = 0; j < n1y; ++j)
+      for (int i = 0; i < n1x; ++i) {
+        const size_t o = (size_t)j * n1x + i;
+        double v = aos9 ? src_dense[o * 9 + k] : src_dense[(size_t)k * n1x * n1y + o];
+        if (shift) v -= w[k] * h->p.rho0;
+        d[(size_t)k * h->g.plane + (size_t)j * h->g.pitch + i] = (T)v;
+      }
+}
+
+template <class T>
+void from_pitched(const std::vector<unsigned char>& buf, double* dst, const lbm_sim* h) {
+  const int n1x = h->p.nx + 1, n1y = h->p.ny + 1;
+  const T* s = reinterpret_cast<const T*>(buf.data());
+  for (int j = 0; j < n1y; ++j)
+    for (int i = 0; i < n1x; ++i) dst[(size_t)j * n1x + i] = (double)s[(size_t)j * h->g.pitch + i];
+}
+
+void destroy_buffers(lbm_sim* h) {
+  for (int b = 0; b < 2; ++b) {
+    dfree(h->f[b]);
+    dfree(h->om[b]);
+  }
+  dfree(h->rec);
+  dfree(h->ps); dfree(h->tbox); dfree(h->partials);
+  dfree(h->cell_count); dfree(h->cell_start); dfree(h->cell_items); dfree(h->cell_of);
+  dfree(h->tile_count); dfree(h->tile_list);
+  dfree(h->ticket); dfree(h->mass_partials); dfree(h->d_kk); dfree(h->stale_dpw);
+  dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
+  if (h->h_status) cudaFreeHost(h->h_status);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_params_init(lbm_params* p) {
+  if (!p) return LBM_E_INVALID;
+  std::memset(p, 0, sizeof(*p));
+  p->struct_size = (int32_t)sizeof(lbm_params);
+  // C1 PARAMETERs as the Fortran holds them (REAL(4) literals widened)
+  const float f1_36 = 1.0f / 36.0f, f1_6 = 1.0f / 6.0f;
+  p->nx = 240;
+  p->ny = 720;
+  p->precision = LBM_FP64;
+  p->bc = LBM_BC_ZOUHE;
+  p->rheology = LBM_NEWTONIAN;
+  p->rate_set = LBM_RATES_FIXED_Q;
+  p->wall_model = LBM_WALL_MIRROR;
+  p->contact_test = LBM_CONTACT_STALE_DPW;
+  p->integrate_angle = 0;
+  p->series_every = 1;
+  p->series_particles = 1;
+  p->series_capacity = 4096;
+  p->record_stress = 0;
+  p->device = 0;
+  p->nu = (double)0.05f;
+  p->rho0 = 1.0;
+  p->s_e = (double)1.1f;
+  p->s_eps = 1.0;
+  p->s_q = (double)1.2f;
+  p->d_mrt = (double)f1_36;
+  p->inv_six = (double)f1_6;
+  p->w_init[0] = (double)(2.0f / 9.0f);
+  p->w_init[1] = (double)(1.0f / 18.0f);
+  p->w_init[2] = (double)(1.0f / 36.0f);
+  p->pi = (double)3.14159265359f;
+  p->zeta = 1.0;
+  const double c_l = (double)0.25f / 30.0;
+  const double c_t = (c_l * c_l) * p->nu / (double)0.1f;
+  const double c_g = c_l * (double)0.01f / (c_t * c_t);
+  p->gravity = -(double)9.81f / c_g;
+  p->tau_y = 1.0 * p->nu * 1.0 / 30.0;
+  p->m_pap = (double)1.0e8f;
+  p->gamma_min = (double)1.0e-15f;
+  p->rep_zeta = 2.0;
+  p->eps_p = 1.0e5;
+  p->eps_w = 0.5 * p->eps_p;
+  p->e_p = 2.0e5;
+  p->e_w = 0.5 * p->e_p;
+  const double D = 30.0;
+  p->c_ij = -((((((double)1.25f - 1.0) * p->gravity) * p->pi) * 0.5) * D * 0.5) * D;
+  const double edge3 = 0.5 * (double)p->ny + 0.5 * (2.0 * (double)p->ny);
+  const double edge4 = 0.5 * (double)p->nx - 0.5 * (2.0 * (double)p->nx);
+  p->wall_mirror_top = 2.0 * edge3;
+  p->wall_mirror_left = 2.0 * edge4;
+  return LBM_OK;
+}
+
+int lbm_create(const lbm_params* pin, lbm_sim** out) {
+  if (!pin || !out) return LBM_E_INVALID;
+  *out = nullptr;
+  if (pin->struct_size != (int32_t)sizeof(lbm_params)) return LBM_E_ABI;
+  const lbm_params& p = *pin;
+  if (p.nx < 2 || p.ny < 2 || (long long)(p.nx + 1) * (p.ny + 1) > (1LL << 31)) return LBM_E_INVALID;
+  if (p.precision != LBM_FP64 && p.precision != LBM_FP32_SHIFTED) return LBM_E_INVALID;
+  if (p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB) return LBM_E_INVALID;
+  if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM) return LBM_E_INVALID;
+  if (p.wall_model < 0 || p.wall_model > 2 || p.contact_test < 0 || p.contact_test > 1)
+    return LBM_E_INVALID;
+  if (!std::isfinite(p.nu) || !(p.rho0 > 0.0) || !(p.zeta > 0.0) || !(p.rep_zeta > 0.0) ||
+      !(p.d_mrt > 0.0))
+    return LBM_E_INVALID;
+  const double omega = 1.0 / (3. * p.nu + 0.5);
+  if (!(1.0 / omega >= 0.5)) return LBM_E_TAU;  // C1:127-130: IF(1.0/OMEGA < 0.5) STOP
+  if (p.series_every < 0 || p.series_capacity < 0 || p.series_particles < 0) return LBM_E_INVALID;
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LBM_E_CUDA;
+  if (p.device < 0 || p.device >= ndev) return LBM_E_INVALID;
+  if (cudaSetDevice(p.device) != cudaSuccess) return LBM_E_CUDA;
+
+  lbm_sim* h = new (std::nothrow) lbm_sim();
+  if (!h) return LBM_E_NOMEM;
+  h->p = p;
+  h->prec = p.precision;
+  h->esz = h->prec == LBM_FP64 ? 8 : 4;
+  h->g.nx = p.nx;
+  h->g.ny = p.ny;
+  h->g.pitch = ((p.nx + 1) + 31) / 32 * 32;
+  h->g.plane = (long long)h->g.pitch * (p.ny + 1);
+  h->g.nbx = (p.nx + 1 + TX - 1) / TX;
+  h->g.nby = (p.ny + 1 + TY - 1) / TY;
+  Model& m = h->m;
+  m.bc = p.bc;
+  m.bingham = p.rheology == LBM_BINGHAM;
+  m.q_of_omega = p.rate_set == LBM_RATES_Q_OF_OMEGA;
+  m.record_stress = p.record_stress ? 1 : 0;
+  m.rho0 = p.rho0;
+  m.nu = p.nu;
+  m.omega = omega;
+  m.s_e = p.s_e;
+  m.s_eps = p.s_eps;
+  m.s_q = p.s_q;
+  m.d_mrt = p.d_mrt;
+  m.pi = p.pi;
+  m.zeta = p.zeta;
+  m.tau_y = p.tau_y;
+  m.m_pap = p.m_pap;
+  m.gamma_min = p.gamma_min;
+  for (int k = 0; k < 3; ++k) m.w_init[k] = p.w_init[k];
+  static const double w[9] = {4.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9,
+                              1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
+  for (int k = 0; k < 9; ++k) m.shift_c[k] = p.rho0 * w[k] * (36.0 * p.d_mrt - 1.0);
+
+  int rc = LBM_OK;
+  auto fail = [&](int code) {
+    destroy_buffers(h);
+    delete h;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(LBM_E_CUDA);
+  if (cudaHostAlloc(reinterpret_cast<void**>(&h->h_status), sizeof(int), cudaHostAllocDefault) !=
+      cudaSuccess)
+    return fail(LBM_E_NOMEM);
+  *h->h_status = 0;
+  if ((rc = dalloc(&h->d_status, 1))) return fail(rc);
+  cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream);
+  const size_t fbytes = (size_t)9 * h->g.plane * h->esz;
+  for (int b = 0; b < 2; ++b) {
+    if (cudaMalloc(&h->f[b], fbytes) != cudaSuccess) return fail(LBM_E_NOMEM);
+    if (m.bingham && cudaMalloc(&h->om[b], (size_t)h->g.plane * h->esz) != cudaSuccess)
+      return fail(LBM_E_NOMEM);
+  }
+  if (m.record_stress &&
+      cudaMalloc(&h->rec, (size_t)2 * 4 * h->g.plane * h->esz) != cudaSuccess)
+    return fail(LBM_E_NOMEM);
+  const int ntiles = h->g.nbx * h->g.nby;
+  if ((rc = dalloc(&h->tile_count, ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->tile_list, (size_t)ntiles * h->tile_cap))) return fail(rc);
+  if ((rc = dalloc(&h->ticket, 1))) return fail(rc);
+  if ((rc = dalloc(&h->mass_partials, ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->d_kk, 1))) return fail(rc);
+  if ((rc = dalloc(&h->stale_dpw, 1))) return fail(rc);
+  if ((rc = dalloc(&h->out, (size_t)NOUT * nodes(h)))) return fail(rc);
+  cudaMemsetAsync(h->f[0], 0, fbytes, h->stream);
+  cudaMemsetAsync(h->f[1], 0, fbytes, h->stream);
+  cudaMemsetAsync(h->tile_count, 0, sizeof(int) * ntiles, h->stream);
+  cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int), h->stream);
+  cudaMemsetAsync(h->d_kk, 0, sizeof(long long), h->stream);
+  const double inf = INFINITY;
+  cudaMemcpyAsync(h->stale_dpw, &inf, sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if ((rc = setup_particle_buffers(h, 0, 0.0))) return fail(rc);
+  // f*(1) = collision of step 1 applied to INITIALIZE's state (C1:151, C1:296)
+  h->cur = 0;
+  LatticeArgs a = lattice_args(h);
+  a.src = nullptr;
+  a.dst = h->f[0];
+  a.om_dst = h->om[0];
+  if (launch_lattice(h, a, 2) != cudaSuccess) return fail(LBM_E_CUDA);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(LBM_E_CUDA);
+  *out = h;
+  return LBM_OK;
+}
+
+int lbm_destroy(lbm_sim* h) {
+  if (!h) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  destroy_buffers(h);
+  delete h;
+  return LBM_OK;
+}
+
+int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
+  if (!h || np < 0 || (np > 0 && !pin)) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  double dmax = 0.0;
+  for (int i = 0; i < np; ++i) {
+    const double* r = pin + (size_t)LBM_PIN * i;
+    for (int k = 0; k < LBM_PIN; ++k)
+      if (!std::isfinite(r[k])) return LBM_E_INVALID;
+    if (!(r[6] > 0.0) || !(r[7] > 0.0)) return LBM_E_INVALID;
+    if (r[0] < 0.0 || r[0] > h->p.nx || r[1] < 0.0 || r[1] > h->p.ny) return LBM_E_PARTICLE;
+    dmax = std::max(dmax, r[6]);
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  int rc = setup_particle_buffers(h, np, dmax);
+  if (rc) return rc;
+  std::vector<double> buf((size_t)std::max(np, 1) * PS, 0.0);
+  for (int i = 0; i < np; ++i) {
+    const double* r = pin + (size_t)LBM_PIN * i;
+    particle_record(h->p, &buf[(size_t)i * PS], r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]);
+  }
+  CK(h2d(h, h->ps, buf.data(), buf.size() * sizeof(double)));
+  if ((rc = launch_tiles(h))) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  h->out_kk = -1;
+  h->drained_kk = h->kk;
+  return refreshed_status(h);
+}
+
+int lbm_step(lbm_sim* h, int32_t nsteps) {
+  if (!h || nsteps < 0) return LBM_E_INVALID;
+  int st = sticky_status(h);
+  if (st) return st;
+  cudaSetDevice(h->p.device);
+  const int every = h->p.series_every;
+  for (int32_t s = 0; s < nsteps; ++s) {
+    if (h->series && every > 0 && (h->kk + 1) / every - h->drained_kk / every > h->series_cap) {
+      int rc = drain_series(h);
+      if (rc) return rc;
+    }
+    ParticleArgs pa = particle_args(h);
+    CK(launch_particles(pa, h->stream));
+    LatticeArgs a = lattice_args(h);
+    CK(launch_lattice(h, a, 0));
+    h->cur ^= 1;
+    h->kk += 1;
+    h->prev_post_bc = false;
+  }
+  h->out_kk = -1;
+  CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  return LBM_OK;
+}
+
+int lbm_get_step(lbm_sim* h, int64_t* kk) {
+  if (!h || !kk) return LBM_E_INVALID;
+  *kk = h->kk;
+  return LBM_OK;
+}
+
+int lbm_get_particles(lbm_sim* h, double* out) {
+  if (!h || (!out && h->np > 0)) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  std::vector<double> buf((size_t)std::max(h->np, 1) * PS);
+  CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
+  for (int i = 0; i < h->np; ++i) {
+    const double* P = &buf[(size_t)i * PS];
+    double* r = out + (size_t)LBM_POUT * i;
+    r[0] = P[P_X]; r[1] = P[P_Y]; r[2] = P[P_ANG];
+    r[3] = P[P_U]; r[4] = P[P_V]; r[5] = P[P_W];
+    r[6] = P[P_FX]; r[7] = P[P_FY]; r[8] = P[P_TZ];
+    r[9] = P[P_FCX]; r[10] = P[P_FCY];
+    r[11] = P[P_FHX]; r[12] = P[P_FHY]; r[13] = P[P_FHT];
+    r[14] = P[P_M]; r[15] = P[P_I];
+  }
+  return refreshed_status(h);
+}
+
+int lbm_get_field(lbm_sim* h, int32_t which, double* out) {
+  if (!h || !out) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  const long long nn = nodes(h);
+  const int n1x = h->p.nx + 1, n1y = h->p.ny + 1;
+  if (which >= LBM_FIELD_UX && which <= LBM_FIELD_GY) {
+    int rc = compute_output(h, false);
+    if (rc) return rc;
+    const int slot = which == LBM_FIELD_UX ? 0 : which == LBM_FIELD_UY ? 1 :
+                     which == LBM_FIELD_RHO ? 2 : which == LBM_FIELD_PHI ? 3 :
+                     which == LBM_FIELD_GX ? 4 : 5;
+    CK(d2h(h, out, h->out + (size_t)slot * nn, nn * sizeof(double)));
+    return refreshed_status(h);
+  }
+  if (which == LBM_FIELD_OMEGA) {
+    if (!h->m.bingham || h->kk == 0) {
+      for (long long i = 0; i < nn; ++i) out[i] = h->m.omega;
+      return LBM_OK;
+    }
+    std::vector<unsigned char> buf((size_t)h->g.plane * h->esz);
+    CK(d2h(h, buf.data(), h->om[h->cur ^ 1], buf.size()));
+    if (h->prec == LBM_FP64) from_pitched<double>(buf, out, h); else from_pitched<float>(buf, out, h);
+    return LBM_OK;
+  }
+  if (which >= LBM_FIELD_TAU11 && which <= LBM_FIELD_TAU12) {
+    if (!h->rec) return LBM_E_STATE;
+    if (h->kk == 0) {
+      for (long long i = 0; i < nn; ++i) out[i] = 0.0;
+      return LBM_OK;
+    }
+    const int slot = (int)(h->kk & 1);
+    const int comp = which - LBM_FIELD_TAU11;
+    std::vector<unsigned char> buf((size_t)h->g.plane * h->esz);
+    const size_t off = ((size_t)slot * 4 + comp) * h->g.plane * h->esz;
+    CK(d2h(h, buf.data(), static_cast<unsigned char*>(h->rec) + off, buf.size()));
+    if (h->prec == LBM_FP64) from_pitched<double>(buf, out, h); else from_pitched<float>(buf, out, h);
+    (void)n1x; (void)n1y;
+    return LBM_OK;
+  }
+  return LBM_E_INVALID;
+}
+
+int lbm_get_image(lbm_sim* h, int32_t* out) {
+  if (!h || !out) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  const long long nn = nodes(h);
+  int rc = compute_output(h, false);
+  if (rc) return rc;
+  std::vector<double> pn(nn), yd;
+  CK(d2h(h, pn.data(), h->out + 6 * nn, nn * sizeof(double)));
+  if (h->m.bingham && h->rec && h->kk > 0) {
+    yd.resize(nn);
+    std::vector<unsigned char> buf((size_t)h->g.plane * h->esz);
+    const size_t off = ((size_t)(h->kk & 1) * 4 + 3) * h->g.plane * h->esz;
+    CK(d2h(h, buf.data(), static_cast<unsigned char*>(h->rec) + off, buf.size()));
+    if (h->prec == LBM_FP64) from_pitched<double>(buf, yd.data(), h);
+    else from_pitched<float>(buf, yd.data(), h);
+  }
+  for (long long i = 0; i < nn; ++i)
+    out[i] = pn[i] > 5.0 ? 10 : (yd.empty() ? 0 : (int32_t)yd[i]);
+  return refreshed_status(h);
+}
+
+int lbm_series_record_len(lbm_sim* h, int32_t* len) {
+  if (!h || !len) return LBM_E_INVALID;
+  *len = h->series_len;
+  return LBM_OK;
+}
+
+int lbm_get_series(lbm_sim* h, double* out, int32_t max_records, int32_t* nrec) {
+  if (!h || !nrec || max_records < 0) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  int rc = drain_series(h);
+  if (rc) return rc;
+  const size_t len = (size_t)h->series_len;
+  const size_t avail = (h->host_series.size() - h->host_series_read) / len;
+  const size_t n = std::min<size_t>(avail, (size_t)max_records);
+  if (n && out)
+    std::memcpy(out, h->host_series.data() + h->host_series_read, n * len * sizeof(double));
+  h->host_series_read += n * len;
+  if (h->host_series_read == h->host_series.size()) {
+    h->host_series.clear();
+    h->host_series_read = 0;
+  }
+  *nrec = (int32_t)n;
+  return refreshed_status(h);
+}
+
+int lbm_get_mean_density(lbm_sim* h, double* avg) {
+  if (!h || !avg) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  const long long nn = nodes(h);
+  int rc = compute_output(h, false);
+  if (rc) return rc;
+  std::vector<double> r(nn);
+  CK(d2h(h, r.data(), h->out + 2 * nn, nn * sizeof(double)));
+  double s = 0.0;
+  for (long long i = 0; i < nn; ++i) s += r[i];
+  *avg = s / (double)nn;
+  return std::isfinite(*avg) ? LBM_OK : LBM_E_NAN;
+}
+
+int lbm_get_state(lbm_sim* h, double* f, double* omega, double* particles) {
+  if (!h) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  const long long nn = nodes(h);
+  if (f) {
+    if (!h->out_f) {
+      int rc = dalloc(&h->out_f, (size_t)9 * nn);
+      if (rc) return rc;
+    }
+    h->out_kk = -1;
+    int rc = compute_output(h, true);
+    if (rc) return rc;
+    CK(d2h(h, f, h->out_f, (size_t)9 * nn * sizeof(double)));
+  }
+  if (omega) {
+    int rc = lbm_get_field(h, LBM_FIELD_OMEGA, omega);
+    if (rc) return rc;
+  }
+  if (particles && h->np > 0) {
+    std::vector<double> buf((size_t)h->np * PS);
+    double stale = 0.0;
+    CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
+    CK(d2h(h, &stale, h->stale_dpw, sizeof(double)));
+    for (int i = 0; i < h->np; ++i) {
+      const double* P = &buf[(size_t)i * PS];
+      double* r = particles + (size_t)LBM_STATE_PER * i;
+      r[0] = P[P_X]; r[1] = P[P_Y]; r[2] = P[P_ANG];
+      r[3] = P[P_U]; r[4] = P[P_V]; r[5] = P[P_W];
+      r[6] = P[P_UO]; r[7] = P[P_VO]; r[8] = P[P_WO];
+      r[9] = P[P_FX]; r[10] = P[P_FY]; r[11] = P[P_TZ];
+      r[12] = P[P_FCX]; r[13] = P[P_FCY];
+      r[14] = P[P_FHX]; r[15] = P[P_FHY]; r[16] = P[P_FHT];
+      r[17] = P[P_D]; r[18] = P[P_RHO]; r[19] = stale;
+    }
+  }
+  return refreshed_status(h);
+}
+
+int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, int32_t np,
+                  const double* particles) {
+  if (!h || !f || kk < 0 || np < 0 || (np > 0 && !particles)) return LBM_E_INVALID;
+  if (h->m.bingham && !omega) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  CK(cudaStreamSynchronize(h->stream));
+  double dmax = 0.0;
+  for (int i = 0; i < np; ++i) {
+    const double* r = particles + (size_t)LBM_STATE_PER * i;
+    if (!(r[17] > 0.0) || !(r[18] > 0.0)) return LBM_E_INVALID;
+    dmax = std::max(dmax, r[17]);
+  }
+  int rc = setup_particle_buffers(h, np, dmax);
+  if (rc) return rc;
+  std::vector<double> buf((size_t)std::max(np, 1) * PS, 0.0);
+  double stale = INFINITY;
+  for (int i = 0; i < np; ++i) {
+    const double* r = particles + (size_t)LBM_STATE_PER * i;
+    double* P = &buf[(size_t)i * PS];
+    particle_record(h->p, P, r[0], r[1], r[2], r[3], r[4], r[5], r[17], r[18]);
+    P[P_UO] = r[6]; P[P_VO] = r[7]; P[P_WO] = r[8];
+    P[P_FX] = r[9]; P[P_FY] = r[10]; P[P_TZ] = r[11];
+    P[P_FCX] = r[12]; P[P_FCY] = r[13];
+    P[P_FHX] = r[14]; P[P_FHY] = r[15]; P[P_FHT] = r[16];
+    stale = r[19];
+  }
+  CK(h2d(h, h->ps, buf.data(), buf.size() * sizeof(double)));
+  CK(h2d(h, h->stale_dpw, &stale, sizeof(double)));
+  const long long kkl = kk;
+  CK(h2d(h, h->d_kk, &kkl, sizeof(long long)));
+  // F after BC of step kk into the "previous" buffer
+  std::vector<unsigned char> pb;
+  const int prev = h->cur ^ 1;
+  if (h->prec == LBM_FP64) to_pitched<double>(f, pb, h, 9, true, false);
+  else to_pitched<float>(f, pb, h, 9, true, true);
+  CK(h2d(h, h->f[prev], pb.data(), pb.size()));
+  CK(cudaStreamSynchronize(h->stream));  // pb is reused below
+  if (h->m.bingham) {
+    if (h->prec == LBM_FP64) to_pitched<double>(omega, pb, h, 1, false, false);
+    else to_pitched<float>(omega, pb, h, 1, false, false);
+    CK(h2d(h, h->om[prev], pb.data(), pb.size()));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  h->kk = kk;
+  h->drained_kk = kk;
+  h->host_series.clear();
+  h->host_series_read = 0;
+  if ((rc = launch_tiles(h))) return rc;
+  // collision of step kk+1 from the restored state
+  LatticeArgs a = lattice_args(h);
+  a.src = h->f[prev];
+  a.om_src = h->om[prev];
+  a.dst = h->f[h->cur];
+  a.om_dst = h->om[h->cur];
+  CK(launch_lattice(h, a, 3));
+  CK(cudaStreamSynchronize(h->stream));
+  h->prev_post_bc = true;
+  h->out_kk = -1;
+  return refreshed_status(h);
+}
+
+int lbm_get_status(lbm_sim* h) {
+  if (!h) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  CK(d2h(h, h->h_status, h->d_status, sizeof(int)));
+  return sticky_status(h);
+}
+
+const char* lbm_strerror(int code) {
+  switch (code) {
+    case LBM_OK: return "ok";
+    case LBM_E_INVALID: return "invalid argument or parameter";
+    case LBM_E_TAU: return "relaxation time exceeded 0.5 -> stability problem";
+    case LBM_E_NOMEM: return "out of memory";
+    case LBM_E_CUDA: return "CUDA error (no device or launch failure)";
+    case LBM_E_NAN: return "non-finite density or particle state";
+    case LBM_E_TIMEOUT: return "bounded device wait expired";
+    case LBM_E_OVERFLOW: return "too many particles touch one lattice tile";
+    case LBM_E_STATE: return "call out of order";
+    case LBM_E_PARTICLE: return "particle outside the lattice";
+    case LBM_E_ABI: return "lbm_params.struct_size mismatch";
+    default: return "unknown error";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,18 @@
+// lbm_fp32.cu -- FP32 shifted-population instantiation of the lattice kernel
+// (h = f - w_k*rho0 stored and computed in FP32; reductions in FP64).
+#include "lbm_lattice.cuh"
+
+namespace lbm {
+cudaError_t launch_init_fp32(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<float>(a, s, MODE_INIT);
+}
+cudaError_t launch_step_fp32(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<float>(a, s, MODE_STEP);
+}
+cudaError_t launch_output_fp32(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<float>(a, s, MODE_OUTPUT);
+}
+cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<float>(a, s, MODE_RESTART);
+}
+}  // namespace lbm

@@ -1,0 +1,20 @@
+// lbm_fp64.cu -- FP64 plain-population instantiation of the lattice kernel.
+// Built with --fmad=false: every product and sum rounds on its own, in the
+// reference's order, so the only differences from the FP64 oracle come from
+// sin() and from the order of the force reductions.
+#include "lbm_lattice.cuh"
+
+namespace lbm {
+cudaError_t launch_init_fp64(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<double>(a, s, MODE_INIT);
+}
+cudaError_t launch_step_fp64(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<double>(a, s, MODE_STEP);
+}
+cudaError_t launch_output_fp64(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<double>(a, s, MODE_OUTPUT);
+}
+cudaError_t launch_restart_fp64(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<double>(a, s, MODE_RESTART);
+}
+}  // namespace lbm

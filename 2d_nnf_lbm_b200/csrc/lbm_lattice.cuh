@@ -1,0 +1,706 @@
+// lbm_lattice.cuh -- the fused lattice kernel of one time step (sm_100a).
+//
+// One launch per time step k does, for every node in one pass over HBM:
+//   pull-stream the stored post-collision populations f*(k)     C1:1181-1217
+//   boundary conditions (Zou-He edges / half-way bounce-back)    C1:1222-1417,
+//                                                                C6:1195-1390
+//   macroscopic rho, u                                           C1:1421-1439
+//   SPM solid fraction and body force G (last particle wins)     C1:407-542
+//   per-tile partial sums of the hydrodynamic force and torque   C1:546-570
+//   velocity correction u += G/2                                 C1:1138-1152
+//   MRT collision of step k+1 (+ Papanastasiou viscosity)        C1:875-1048,
+//                                                                C6:867-1021
+// and writes f*(k+1).  The collision of step k+1 only reads quantities of
+// step k (rho, corrected u, G, per-node omega), which is why it can run in the
+// same pass as the streaming of step k (C1:292-315 data flow).  The last
+// block to finish reduces the per-tile partials into each particle's FORCE
+// in a fixed order, so results do not depend on block scheduling.
+//
+// Precision policies:
+//   double -- plain populations f, operation order of the reference; the TU
+//             is compiled with --fmad=false so products are not contracted.
+//   float  -- shifted populations h = f - w_k*rho0 in FP32, FP32 arithmetic;
+//             force/torque/mass reductions in FP64.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+enum { MODE_STEP = 0, MODE_OUTPUT = 1, MODE_INIT = 2, MODE_RESTART = 3 };
+
+// exact D2Q9 weights for the shift of the FP32 representation
+__device__ __forceinline__ double wexact(int k) {
+  return k == 0 ? 4.0 / 9.0 : (k < 5 ? 1.0 / 9.0 : 1.0 / 36.0);
+}
+
+// ---------------------------------------------------------------------------
+// COMPUTEFEQNEW (C1:1157-1175) in double.
+__device__ __forceinline__ void feq_double(const Model& m, double ux, double uy, double rho,
+                                           double* feq) {
+  const double W0 = m.w_init[0], W1 = m.w_init[1], W2 = m.w_init[2];
+  const double U2 = ux * ux + uy * uy;
+  feq[0] = W0 * rho * (2. - 3. * U2);
+  feq[1] = W1 * rho * (2. + 6. * ux + 9. * ux * ux - 3. * U2);
+  feq[2] = W1 * rho * (2. + 6. * uy + 9. * uy * uy - 3. * U2);
+  feq[3] = W1 * rho * (2. - 6. * ux + 9. * ux * ux - 3. * U2);
+  feq[4] = W1 * rho * (2. - 6. * uy + 9. * uy * uy - 3. * U2);
+  feq[5] = W2 * rho * (1. + 3. * (ux + uy) + 9. * ux * uy + 3. * U2);
+  feq[6] = W2 * rho * (1. - 3. * (ux - uy) - 9. * ux * uy + 3. * U2);
+  feq[7] = W2 * rho * (1. - 3. * (ux + uy) + 9. * ux * uy + 3. * U2);
+  feq[8] = W2 * rho * (1. + 3. * (ux - uy) - 9. * ux * uy + 3. * U2);
+}
+
+// ComputeRelaxation_MRT (C1:1029-1048 fixed q; C6:1002-1021 q of omega).
+__device__ __forceinline__ void rates_double(const Model& m, double omega, double* S) {
+  const double oq = m.q_of_omega ? 8. * (2. - omega) / (8. - omega) : m.s_q;
+  S[0] = 0.0; S[1] = m.s_e; S[2] = m.s_eps; S[3] = 0.0;
+  S[4] = oq; S[5] = 0.0; S[6] = oq; S[7] = omega; S[8] = omega;
+}
+
+// ---------------------------------------------------------------------------
+// SPM solid fraction of one node for one disk (C1:464-476).
+__device__ __forceinline__ double phi_double(double di, double dj, double R, double zeta,
+                                             double pi) {
+  const double D = R - sqrt(di * di + dj * dj);
+  double phi = 0.0;
+  if (D <= -0.5 * zeta)
+    phi = 0.0;
+  else if (fabs(D) < 0.5 * zeta)
+    phi = 0.5 * (sin(pi * D / zeta) + 1.0);
+  else if (D >= 0.5 * zeta)
+    phi = 1.0;
+  return phi;
+}
+
+__device__ __forceinline__ float phi_float(float di, float dj, float R, float zeta, float pi) {
+  const float D = R - sqrtf(di * di + dj * dj);
+  float phi = 0.0f;
+  if (D <= -0.5f * zeta)
+    phi = 0.0f;
+  else if (fabsf(D) < 0.5f * zeta)
+    phi = 0.5f * (sinf(pi * D / zeta) + 1.0f);
+  else if (D >= 0.5f * zeta)
+    phi = 1.0f;
+  return phi;
+}
+
+// ---------------------------------------------------------------------------
+// Collision_MRT for one node in plain FP64 (C1:886-921; Chai strain rate and
+// Papanastasiou viscosity C6:903-958).  Same operations, same order as the
+// reference.  Returns the new omega and writes stress / yield code.
+struct NodeOut {
+  double t11, t22, t12, omega;
+  int yield;
+};
+
+__device__ __forceinline__ void collide_double(const Model& m, double* f, double RHO, double UX,
+                                               double UY, double GX, double GY, const double* S,
+                                               bool want_stress, NodeOut& no) {
+  const double d_mrt = m.d_mrt;
+  const double f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3], f4 = f[4], f5 = f[5], f6 = f[6],
+               f7 = f[7], f8 = f[8];
+  double M[9], MF[9], MEQ[9];
+  M[0] = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8;
+  M[1] = -4.0 * f0 - f1 - f2 - f3 - f4 + 2.0 * (f5 + f6 + f7 + f8);
+  M[2] = 4.0 * f0 - 2.0 * (f1 + f2 + f3 + f4) + (f5 + f6 + f7 + f8);
+  M[3] = f1 - f3 + f5 - f6 - f7 + f8;
+  M[4] = -2.0 * (f1 - f3) + f5 - f6 - f7 + f8;
+  M[5] = f2 - f4 + f5 + f6 - f7 - f8;
+  M[6] = -2.0 * (f2 - f4) + f5 + f6 - f7 - f8;
+  M[7] = f1 - f2 + f3 - f4;
+  M[8] = f5 - f6 + f7 - f8;
+  const double F_X = RHO * (GX + 0.0), F_Y = RHO * (GY + 0.0);
+  MF[0] = 0.0;
+  MF[1] = 6.0 * (F_X * UX + F_Y * UY);
+  MF[2] = -6.0 * (F_X * UX + F_Y * UY);
+  MF[3] = F_X;
+  MF[4] = -F_X;
+  MF[5] = F_Y;
+  MF[6] = -F_Y;
+  MF[7] = 2.0 * (F_X * UX - F_Y * UY);
+  MF[8] = F_Y * UX + F_X * UY;
+  const double U2 = UX * UX + UY * UY;
+  MEQ[0] = RHO;
+  MEQ[1] = RHO * (-2.0 + 3. * U2);
+  MEQ[2] = RHO * (1.0 - 3. * U2);
+  MEQ[3] = RHO * (UX);
+  MEQ[4] = RHO * (-UX);
+  MEQ[5] = RHO * (UY);
+  MEQ[6] = RHO * (-UY);
+  MEQ[7] = RHO * (UX * UX - UY * UY);
+  MEQ[8] = RHO * (UX * UY);
+  double mm[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k)
+    mm[k] = S[k] * MEQ[k] + (1. - S[k]) * M[k] + (1. - 0.5 * S[k]) * MF[k];
+  f[0] = d_mrt * (4.0 * (mm[0] - mm[1] + mm[2]));
+  f[1] = d_mrt * (4. * mm[0] - mm[1] - 2. * mm[2] + 6. * mm[3] - 6. * mm[4] + 9. * mm[7]);
+  f[2] = d_mrt * (4.0 * mm[0] - mm[1] - 2.0 * mm[2] + 6.0 * mm[5] - 6.0 * mm[6] - 9.0 * mm[7]);
+  f[3] = d_mrt * (4.0 * mm[0] - mm[1] - 2.0 * mm[2] - 6.0 * mm[3] + 6.0 * mm[4] + 9.0 * mm[7]);
+  f[4] = d_mrt * (4.0 * mm[0] - mm[1] - 2.0 * mm[2] - 6.0 * mm[5] + 6.0 * mm[6] - 9.0 * mm[7]);
+  f[5] = d_mrt * (4.0 * mm[0] + 2.0 * mm[1] + mm[2] + 6.0 * mm[3] + 3.0 * mm[4] + 6.0 * mm[5] +
+                  3.0 * mm[6] + 9.0 * mm[8]);
+  f[6] = d_mrt * (4.0 * mm[0] + 2.0 * mm[1] + mm[2] - 6.0 * mm[3] - 3.0 * mm[4] + 6.0 * mm[5] +
+                  3.0 * mm[6] - 9.0 * mm[8]);
+  f[7] = d_mrt * (4.0 * mm[0] + 2.0 * mm[1] + mm[2] - 6.0 * mm[3] - 3.0 * mm[4] - 6.0 * mm[5] -
+                  3.0 * mm[6] + 9.0 * mm[8]);
+  f[8] = d_mrt * (4.0 * mm[0] + 2.0 * mm[1] + mm[2] + 6.0 * mm[3] + 3.0 * mm[4] - 6.0 * mm[5] -
+                  3.0 * mm[6] - 9.0 * mm[8]);
+  if (!want_stress) return;
+  // Chai strain rate from S*(m - m_eq) + forcing correction, C6:903-916
+  double MNE[9], F1[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) MNE[k] = M[k] - MEQ[k];
+  F1[1] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] -
+          6.0 * S[4] * MNE[4] + 9.0 * S[7] * MNE[7];
+  F1[2] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] + 6.0 * S[5] * MNE[5] -
+          6.0 * S[6] * MNE[6] - 9.0 * S[7] * MNE[7];
+  F1[3] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] - 6.0 * S[3] * MNE[3] +
+          6.0 * S[4] * MNE[4] + 9.0 * S[7] * MNE[7];
+  F1[4] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] - 6.0 * S[5] * MNE[5] +
+          6.0 * S[6] * MNE[6] - 9.0 * S[7] * MNE[7];
+  F1[5] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] +
+          3.0 * S[4] * MNE[4] + 6.0 * S[5] * MNE[5] + 3.0 * S[6] * MNE[6] + 9.0 * S[8] * MNE[8];
+  F1[6] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] - 6.0 * S[3] * MNE[3] -
+          3.0 * S[4] * MNE[4] + 6.0 * S[5] * MNE[5] + 3.0 * S[6] * MNE[6] - 9.0 * S[8] * MNE[8];
+  F1[7] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] - 6.0 * S[3] * MNE[3] -
+          3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] + 9.0 * S[8] * MNE[8];
+  F1[8] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] +
+          3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] - 9.0 * S[8] * MNE[8];
+  const double ZARIB = -1.5 * d_mrt;
+  double D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]) +
+               0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
+  double D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]) +
+               0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
+  double D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
+  const double NU = m.nu;
+  no.t11 = NU * 2.0 * D11;
+  no.t22 = NU * 2.0 * D22;
+  no.t12 = NU * 2.0 * D12;
+  no.yield = 0;
+  no.omega = S[7];
+  if (m.bingham) {
+    const double INV_RHO = 1.0 / RHO;
+    D11 = D11 * INV_RHO;
+    D22 = D22 * INV_RHO;
+    D12 = D12 * INV_RHO;
+    const double GAMMA = sqrt(2.0 * fabs(D11 * D11 + D22 * D22 + 2.0 * (D12 * D12)));
+    double NU_A;
+    if (GAMMA < m.gamma_min)
+      NU_A = NU + m.m_pap * m.tau_y;
+    else
+      NU_A = NU + (m.tau_y / GAMMA) * (1.0 - exp(-(m.m_pap * GAMMA)));
+    no.t11 = NU_A * 2.0 * D11;
+    no.t22 = NU_A * 2.0 * D22;
+    no.t12 = NU_A * 2.0 * D12;
+    const double TAU_MAG =
+        sqrt(0.5 * fabs(no.t11 * no.t11 + no.t22 * no.t22 + 2.0 * (no.t12 * no.t12)));
+    no.yield = (TAU_MAG <= m.tau_y) ? 5 : 0;
+    NU_A = NU_A * INV_RHO;
+    no.omega = 1.0 / (3.0 * NU_A + 0.5);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same collision on shifted FP32 populations h = f - w*rho0.  Moments of
+// h are m - rho0*(1,-2,1,0,...); the shift cancels in m - m_eq, and the
+// inverse transform adds back rho0*w_k*(36*d_mrt - 1) (zero for exact 1/36).
+struct Rates32 {
+  float s1, s2, sq, sw;
+};
+
+__device__ __forceinline__ void collide_float(const Model& m, float* h, float drho, float rho,
+                                              float ux, float uy, float gx, float gy,
+                                              const Rates32& r, float dmrt, const float* shc,
+                                              bool want_stress, NodeOut& no) {
+  const float h0 = h[0], h1 = h[1], h2 = h[2], h3 = h[3], h4 = h[4], h5 = h[5], h6 = h[6],
+              h7 = h[7], h8 = h[8];
+  const float a1 = (h1 + h2) + (h3 + h4);
+  const float a5 = (h5 + h6) + (h7 + h8);
+  const float m1 = -4.0f * h0 - a1 + 2.0f * a5;
+  const float m2 = 4.0f * h0 - 2.0f * a1 + a5;
+  const float qx = (h5 - h6) - (h7 - h8);
+  const float qy = (h5 + h6) - (h7 + h8);
+  const float jx = (h1 - h3) + qx;
+  const float m4 = -2.0f * (h1 - h3) + qx;
+  const float jy = (h2 - h4) + qy;
+  const float m6 = -2.0f * (h2 - h4) + qy;
+  const float m7 = (h1 + h3) - (h2 + h4);
+  const float m8 = (h5 + h7) - (h6 + h8);
+  const float u2 = ux * ux + uy * uy;
+  const float ru2 = 3.0f * rho * u2;
+  const float e1 = -2.0f * drho + ru2;
+  const float e2 = drho - ru2;
+  const float e4 = -rho * ux;
+  const float e6 = -rho * uy;
+  const float e7 = rho * (ux * ux - uy * uy);
+  const float e8 = rho * (ux * uy);
+  const float FX = rho * gx, FY = rho * gy;
+  const float fu = FX * ux + FY * uy;
+  const float p0 = h0 + a1 + a5;  // conserved: post-collision mass = sum of populations
+  const float p1 = m1 + r.s1 * (e1 - m1) + (1.0f - 0.5f * r.s1) * (6.0f * fu);
+  const float p2 = m2 + r.s2 * (e2 - m2) - (1.0f - 0.5f * r.s2) * (6.0f * fu);
+  const float p3 = jx + FX;
+  const float p4 = m4 + r.sq * (e4 - m4) - (1.0f - 0.5f * r.sq) * FX;
+  const float p5 = jy + FY;
+  const float p6 = m6 + r.sq * (e6 - m6) - (1.0f - 0.5f * r.sq) * FY;
+  const float cw = 1.0f - 0.5f * r.sw;
+  const float p7 = m7 + r.sw * (e7 - m7) + cw * (2.0f * (FX * ux - FY * uy));
+  const float p8 = m8 + r.sw * (e8 - m8) + cw * (FY * ux + FX * uy);
+  const float b = 4.0f * p0 - p1 - 2.0f * p2;
+  const float c = 4.0f * p0 + 2.0f * p1 + p2;
+  const float x3 = 6.0f * p3 - 6.0f * p4;
+  const float y5 = 6.0f * p5 - 6.0f * p6;
+  const float d3 = 6.0f * p3 + 3.0f * p4;
+  const float d5 = 6.0f * p5 + 3.0f * p6;
+  h[0] = dmrt * (4.0f * (p0 - p1 + p2)) + shc[0];
+  h[1] = dmrt * (b + x3 + 9.0f * p7) + shc[1];
+  h[2] = dmrt * (b + y5 - 9.0f * p7) + shc[2];
+  h[3] = dmrt * (b - x3 + 9.0f * p7) + shc[3];
+  h[4] = dmrt * (b - y5 - 9.0f * p7) + shc[4];
+  h[5] = dmrt * (c + d3 + d5 + 9.0f * p8) + shc[5];
+  h[6] = dmrt * (c - d3 + d5 - 9.0f * p8) + shc[6];
+  h[7] = dmrt * (c - d3 - d5 + 9.0f * p8) + shc[7];
+  h[8] = dmrt * (c + d3 - d5 - 9.0f * p8) + shc[8];
+  if (!want_stress) return;
+  // D_ab = -d_mrt*1.5*sum_k c_a c_b [M^-1 S (m - m_eq)]_k*36 + forcing terms;
+  // closed form of C6:903-916 for S0 = S3 = S5 = 0
+  const float n1 = m1 - e1, n7 = m7 - e7, n8 = m8 - e8;
+  const float t1 = 9.0f * r.s1 * n1, t7 = 27.0f * r.sw * n7;
+  const float gu = gx * ux + gy * uy;
+  float D11 = -dmrt * (t1 + t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gx * ux));
+  float D22 = -dmrt * (t1 - t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gy * uy));
+  float D12 = -54.0f * dmrt * r.sw * n8 + 0.75f * (-r.sw * (gx * uy + gy * ux));
+  const float NU = (float)m.nu;
+  no.t11 = NU * 2.0f * D11;
+  no.t22 = NU * 2.0f * D22;
+  no.t12 = NU * 2.0f * D12;
+  no.yield = 0;
+  no.omega = r.sw;
+  if (m.bingham) {
+    const float inv_rho = 1.0f / rho;
+    D11 *= inv_rho;
+    D22 *= inv_rho;
+    D12 *= inv_rho;
+    const float gam = sqrtf(2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12)));
+    const float ty = (float)m.tau_y;
+    float nua;
+    if (gam < (float)m.gamma_min)
+      nua = NU + (float)m.m_pap * ty;
+    else
+      nua = NU + (ty / gam) * (1.0f - expf(-((float)m.m_pap * gam)));
+    const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
+    no.t11 = t11;
+    no.t22 = t22;
+    no.t12 = t12;
+    const float tm = sqrtf(0.5f * fabsf(t11 * t11 + t22 * t22 + 2.0f * (t12 * t12)));
+    no.yield = (tm <= ty) ? 5 : 0;
+    no.omega = 1.0f / (3.0f * (nua * inv_rho) + 0.5f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pull streaming + boundary conditions for one node.  Sources outside the
+// lattice keep the node's own post-collision value (C1:1195-1199); the
+// boundary routine then overwrites the unknowns.  Wall velocities are zero
+// in every reference case, which reduces the moving-wall terms to +-0.
+template <class T>
+__device__ __forceinline__ void pull_bc(const T* __restrict__ src, const Geometry& g, int bc,
+                                        int i, int j, T* f) {
+  const long long P = g.plane;
+  const long long n = (long long)j * g.pitch + i;
+  const int pt = g.pitch;
+  const bool L = (i == 0), R = (i == g.nx), B = (j == 0), U = (j == g.ny);
+  f[0] = src[n];
+  f[1] = !L ? src[P + n - 1] : src[P + n];
+  f[2] = !B ? src[2 * P + n - pt] : src[2 * P + n];
+  f[3] = !R ? src[3 * P + n + 1] : src[3 * P + n];
+  f[4] = !U ? src[4 * P + n + pt] : src[4 * P + n];
+  f[5] = (!L && !B) ? src[5 * P + n - pt - 1] : src[5 * P + n];
+  f[6] = (!R && !B) ? src[6 * P + n - pt + 1] : src[6 * P + n];
+  f[7] = (!R && !U) ? src[7 * P + n + pt + 1] : src[7 * P + n];
+  f[8] = (!L && !U) ? src[8 * P + n + pt - 1] : src[8 * P + n];
+  if (!(L || R || B || U)) return;
+  // own post-collision populations F_POST(k,i,j)
+#define FPOST(k) src[(k) * P + n]
+  if ((L || R) && (B || U)) {
+    // corners: half-way bounce-back of 3 of the 5 unknowns (C1:1390-1414)
+    if (L && B) { f[1] = FPOST(3); f[5] = FPOST(7); f[2] = FPOST(4); }
+    else if (L && U) { f[1] = FPOST(3); f[8] = FPOST(6); f[4] = FPOST(2); }
+    else if (R && U) { f[3] = FPOST(1); f[7] = FPOST(5); f[4] = FPOST(2); }
+    else { f[2] = FPOST(4); f[6] = FPOST(8); f[3] = FPOST(1); }
+    return;
+  }
+  if (bc == 1 /* LBM_BC_HALFWAY_BB, C6:1206-1219, C6:1285-1294 */) {
+    if (U) { f[8] = FPOST(6); f[4] = FPOST(2); f[7] = FPOST(5); }
+    else if (B) { f[5] = FPOST(7); f[2] = FPOST(4); f[6] = FPOST(8); }
+    else if (R) { f[6] = FPOST(8); f[3] = FPOST(1); f[7] = FPOST(5); }
+    else { f[5] = FPOST(7); f[1] = FPOST(3); f[8] = FPOST(6); }
+  } else { /* Zou-He, C1:1250-1258 (top/bottom), C1:1341-1363 (left/right) */
+    if (U) {
+      f[4] = f[2];
+      f[8] = f[6] - (T)0.5 * (f[1] - f[3]);
+      f[7] = f[5] + (T)0.5 * (f[1] - f[3]);
+    } else if (B) {
+      f[2] = f[4];
+      f[5] = f[7] - (T)0.5 * (f[1] - f[3]);
+      f[6] = f[8] + (T)0.5 * (f[1] - f[3]);
+    } else if (L) {
+      f[5] = f[7] - (T)0.5 * (f[2] - f[4]);
+      f[8] = f[6] + (T)0.5 * (f[2] - f[4]);
+      f[1] = f[3];
+    } else {
+      f[6] = f[8] - (T)0.5 * (f[2] - f[4]);
+      f[7] = f[5] + (T)0.5 * (f[2] - f[4]);
+      f[3] = f[1];
+    }
+  }
+#undef FPOST
+}
+
+template <class T>
+__device__ __forceinline__ void pull_interior(const T* __restrict__ src, const Geometry& g,
+                                              long long n, T* f) {
+  const long long P = g.plane;
+  const int pt = g.pitch;
+  f[0] = src[n];
+  f[1] = src[P + n - 1];
+  f[2] = src[2 * P + n - pt];
+  f[3] = src[3 * P + n + 1];
+  f[4] = src[4 * P + n + pt];
+  f[5] = src[5 * P + n - pt - 1];
+  f[6] = src[6 * P + n - pt + 1];
+  f[7] = src[7 * P + n + pt + 1];
+  f[8] = src[8 * P + n + pt - 1];
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic block sum of three doubles (fixed shuffle tree, then warps in
+// order).  All threads of the block must call it.
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double (*red)[4],
+                                           int tid) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if ((tid & 31) == 0) {
+    red[tid >> 5][0] = a;
+    red[tid >> 5][1] = b;
+    red[tid >> 5][2] = c;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double sa = 0.0, sb = 0.0, sc = 0.0;
+#pragma unroll
+    for (int w = 0; w < TPB / 32; ++w) {
+      sa += red[w][0];
+      sb += red[w][1];
+      sc += red[w][2];
+    }
+    a = sa;
+    b = sb;
+    c = sc;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+template <class T, int MODE>
+__global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
+  constexpr bool F64 = sizeof(T) == 8;
+  __shared__ int s_n;
+  __shared__ int s_idx[MAX_TILE_CAND];
+  __shared__ double s_px[MAX_TILE_CAND], s_py[MAX_TILE_CAND], s_pr[MAX_TILE_CAND];
+  __shared__ double s_pu[MAX_TILE_CAND], s_pv[MAX_TILE_CAND], s_pw[MAX_TILE_CAND];
+  __shared__ int4 s_tb[MAX_TILE_CAND];
+  __shared__ double s_red[TPB / 32][4];
+  __shared__ long long s_kk;
+  __shared__ int s_last;
+
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * TX + (tid & (TX - 1));
+  const int j = blockIdx.y * TY + tid / TX;
+  const int tile = blockIdx.y * a.g.nbx + blockIdx.x;
+  const Geometry& g = a.g;
+  const Model& m = a.m;
+
+  if (tid == 0) {
+    int c = 0;
+    if (MODE != MODE_INIT) {
+      c = a.tile_count[tile];
+      if (c > a.tile_cap) {
+        atomicOr(a.status, ST_OVERFLOW);
+        c = a.tile_cap;
+      }
+      for (int k = 0; k < c; ++k) {  // ascending particle index: last one wins G
+        const int v = a.tile_list[(long long)tile * a.tile_cap + k];
+        int q = k;
+        while (q > 0 && s_idx[q - 1] > v) {
+          s_idx[q] = s_idx[q - 1];
+          --q;
+        }
+        s_idx[q] = v;
+      }
+    }
+    s_n = c;
+    s_kk = (MODE == MODE_STEP || MODE == MODE_RESTART) ? *a.kk : 0;
+  }
+  __syncthreads();
+  const int ncand = s_n;
+  if (tid < ncand) {
+    const double* p = a.ps + (long long)s_idx[tid] * PS;
+    s_px[tid] = p[P_X];
+    s_py[tid] = p[P_Y];
+    s_pr[tid] = 0.5 * p[P_D];
+    s_pu[tid] = p[P_U];
+    s_pv[tid] = p[P_V];
+    s_pw[tid] = p[P_W];
+    s_tb[tid] = a.tbox[s_idx[tid]];
+  }
+  __syncthreads();
+
+  const bool act = (i <= g.nx) && (j <= g.ny);
+  const long long n = (long long)j * g.pitch + i;
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  const bool initial = (MODE == MODE_INIT) || (MODE == MODE_OUTPUT && a.initial);
+
+  // ---- populations after streaming and boundary conditions -------------
+  T f[9];
+  if (act) {
+    if (initial) {
+      double feq[9];
+      feq_double(m, 0.0, 0.0, m.rho0, feq);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = F64 ? (T)feq[k] : (T)(feq[k] - wexact(k) * m.rho0);
+    } else if (MODE == MODE_RESTART || (MODE == MODE_OUTPUT && a.src_post_bc)) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = src[k * g.plane + n];
+    } else {
+      const bool interior = blockIdx.x > 0 && blockIdx.y > 0 &&
+                            (int)(blockIdx.x + 1) * TX <= g.nx &&
+                            (int)(blockIdx.y + 1) * TY <= g.ny;
+      if (interior)
+        pull_interior<T>(src, g, n, f);
+      else
+        pull_bc<T>(src, g, m.bc, i, j, f);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (T)0;
+  }
+
+  // ---- macroscopic variables (C1:1421-1439) ----------------------------
+  T rho, drho, ux, uy;
+  if (initial) {
+    rho = (T)m.rho0;
+    drho = (T)0;
+    ux = (T)0;
+    uy = (T)0;
+  } else if (F64) {
+    rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    drho = rho;
+    const T rinv = (T)1.0 / rho;
+    ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
+    uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
+  } else {
+    drho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+    rho = (T)m.rho0 + drho;
+    const T rinv = (T)1.0 / rho;
+    ux = rinv * ((f[1] + f[5] + f[8]) - (f[6] + f[3] + f[7]));
+    uy = rinv * ((f[5] + f[2] + f[6]) - (f[7] + f[4] + f[8]));
+  }
+  if (!act) {
+    rho = (T)1;
+    ux = uy = (T)0;
+  }
+
+  // ---- SPM: G (last particle with PHI>0 wins) and force partials --------
+  T gx = (T)0, gy = (T)0;
+  double phisum = 0.0;
+  bool pnode = false;
+  if (MODE != MODE_INIT) {
+    for (int c = 0; c < ncand; ++c) {
+      double fx = 0.0, fy = 0.0, tz = 0.0;
+      if (act) {
+        const double di = (double)i - s_px[c];
+        const double dj = (double)j - s_py[c];
+        T phi;
+        if (F64)
+          phi = (T)phi_double(di, dj, s_pr[c], m.zeta, m.pi);
+        else
+          phi = (T)phi_float((float)di, (float)dj, (float)s_pr[c], (float)m.zeta, (float)m.pi);
+        if (phi > (T)0) {
+          const T uxp = (T)s_pu[c] - (T)s_pw[c] * (T)dj;
+          const T uyp = (T)s_pv[c] + (T)s_pw[c] * (T)di;
+          if (!initial) {
+            gx = phi * (uxp - ux);
+            gy = phi * (uyp - uy);
+          }
+          if (MODE == MODE_STEP) {
+            const T rp = rho * phi;
+            fx = (double)(rp * (ux - uxp));
+            fy = (double)(rp * (uy - uyp));
+            tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
+          }
+          phisum += (double)phi;
+          if (phi >= (T)0.5) pnode = true;
+        }
+      }
+      if (MODE == MODE_STEP) {
+        block_sum3(fx, fy, tz, s_red, tid);
+        if (tid == 0) {
+          const int4 tb = s_tb[c];
+          const int slot = (blockIdx.y - tb.y) * tb.z + (blockIdx.x - tb.x);
+          double* dstp = a.partials + ((long long)s_idx[c] * a.max_slots + slot) * 3;
+          dstp[0] = fx;
+          dstp[1] = fy;
+          dstp[2] = tz;
+        }
+      }
+    }
+  }
+
+  // ---- velocity correction (C1:1138-1152) --------------------------------
+  const T uxc = ux + (T)0.5 * (gx + (T)0.0);
+  const T uyc = uy + (T)0.5 * (gy + (T)0.0);
+
+  if (MODE == MODE_OUTPUT) {
+    if (act) {
+      const long long nn = (long long)(g.nx + 1) * (g.ny + 1);
+      const long long o = (long long)j * (g.nx + 1) + i;
+      a.out[o] = (double)uxc;
+      a.out[nn + o] = (double)uyc;
+      a.out[2 * nn + o] = F64 ? (double)rho : m.rho0 + (double)drho;
+      a.out[3 * nn + o] = phisum;
+      a.out[4 * nn + o] = (double)gx;
+      a.out[5 * nn + o] = (double)gy;
+      a.out[6 * nn + o] = pnode ? 10.0 : 0.0;
+      if (a.out_f) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+          a.out_f[o * 9 + k] = F64 ? (double)f[k] : (double)f[k] + wexact(k) * m.rho0;
+      }
+    }
+    return;
+  }
+
+  // ---- collision of the next step ---------------------------------------
+  NodeOut no;
+  no.omega = m.omega;
+  no.yield = 0;
+  no.t11 = no.t22 = no.t12 = 0.0;
+  const bool want_stress = m.bingham || m.record_stress;
+  if (act) {
+    double omega_node = m.omega;
+    if (m.bingham && MODE != MODE_INIT) omega_node = (double)static_cast<const T*>(a.om_src)[n];
+    if (F64) {
+      double S[9];
+      rates_double(m, omega_node, S);
+      double fd[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) fd[k] = (double)f[k];
+      collide_double(m, fd, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, S,
+                     want_stress, no);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = (T)fd[k];
+    } else {
+      Rates32 r;
+      r.s1 = (float)m.s_e;
+      r.s2 = (float)m.s_eps;
+      const float w = (float)omega_node;
+      r.sw = w;
+      r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : (float)m.s_q;
+      float sh[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) sh[k] = (float)m.shift_c[k];
+      float hf[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) hf[k] = (float)f[k];
+      collide_float(m, hf, (float)drho, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy,
+                    r, (float)m.d_mrt, sh, want_stress, no);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
+    }
+    T* __restrict__ dst = static_cast<T*>(a.dst);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dst[k * g.plane + n] = f[k];
+    if (m.bingham) static_cast<T*>(a.om_dst)[n] = (T)no.omega;
+    if (m.record_stress) {
+      const int slot = (int)((s_kk + 1) & 1);
+      T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * g.plane;
+      rec[n] = (T)no.t11;
+      rec[g.plane + n] = (T)no.t22;
+      rec[2 * g.plane + n] = (T)no.t12;
+      rec[3 * g.plane + n] = (T)no.yield;
+    }
+  }
+  if (MODE != MODE_STEP) return;
+
+  // ---- mean density at history steps (C1:318) ----------------------------
+  const long long kk = s_kk;
+  const bool rec_step = a.series_every > 0 && (kk % a.series_every) == 0 && a.series != nullptr;
+  const int nblocks = gridDim.x * gridDim.y;
+  if (rec_step) {
+    double s0 = act ? (F64 ? (double)rho : (double)drho) : 0.0, s1 = 0.0, s2 = 0.0;
+    block_sum3(s0, s1, s2, s_red, tid);
+    if (tid == 0) a.mass_partials[tile] = s0;
+  }
+
+  // ---- last block: fixed-order reduction of FORCE and mass ---------------
+  if (tid == 0) {
+    __threadfence();
+    const unsigned int t = atomicAdd(a.ticket, 1u);
+    s_last = (t == (unsigned int)(nblocks - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int p = tid; p < a.np; p += TPB) {
+    const int4 tb = a.tbox[p];
+    const double* pp = a.partials + (long long)p * a.max_slots * 3;
+    double fx = 0.0, fy = 0.0, tz = 0.0;
+    const int ns = tb.z * tb.w;
+    for (int s = 0; s < ns; ++s) {
+      fx += __ldcg(pp + 3 * s);
+      fy += __ldcg(pp + 3 * s + 1);
+      tz += __ldcg(pp + 3 * s + 2);
+    }
+    double* q = a.ps_force + (long long)p * PS;
+    q[P_FX] = fx;
+    q[P_FY] = fy;
+    q[P_TZ] = tz;
+    if (!isfinite(fx) || !isfinite(fy) || !isfinite(tz)) atomicOr(a.status, ST_NAN);
+  }
+  if (rec_step) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int b = tid; b < nblocks; b += TPB) s0 += __ldcg(a.mass_partials + b);
+    block_sum3(s0, s1, s2, s_red, tid);
+    if (tid == 0) {
+      const double nn = (double)((long long)(g.nx + 1) * (g.ny + 1));
+      const double avg = F64 ? s0 / nn : m.rho0 + s0 / nn;
+      const long long r = (kk / a.series_every - 1) % a.series_cap;
+      a.series[r * a.series_len + 1] = avg;
+      if (!isfinite(avg)) atomicOr(a.status, ST_NAN);
+    }
+  }
+  if (tid == 0) *a.ticket = 0u;
+}
+
+template <class T>
+cudaError_t launch_mode(const LatticeArgs& a, cudaStream_t s, int mode) {
+  dim3 grid(a.g.nbx, a.g.nby);
+  switch (mode) {
+    case MODE_STEP: k_lattice<T, MODE_STEP><<<grid, TPB, 0, s>>>(a); break;
+    case MODE_OUTPUT: k_lattice<T, MODE_OUTPUT><<<grid, TPB, 0, s>>>(a); break;
+    case MODE_INIT: k_lattice<T, MODE_INIT><<<grid, TPB, 0, s>>>(a); break;
+    default: k_lattice<T, MODE_RESTART><<<grid, TPB, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace lbm

@@ -1,0 +1,206 @@
+/*
+ * lbm2d.h -- C ABI of the B200 (sm_100a) hot path of 2D_NNF_LBM.
+ *
+ * One handle = one simulation: a D2Q9 MRT lattice of (NX+1) x (NY+1) nodes
+ * (nodes 0..NX, 0..NY, i fastest), rigid disks coupled by the smoothed
+ * profile method (SPM), Glowinski soft-sphere repulsion and an explicit
+ * Newton-Euler particle update.  The library owns all device memory; the
+ * caller owns every host buffer it passes.  Every entry point returns
+ * LBM_OK (0) or a negative LBM_E* code.  A handle is used by one host
+ * thread at a time.  lbm_step() is asynchronous on the handle's own CUDA
+ * stream; every lbm_get_* call synchronises that stream first.
+ *
+ * Reference interface replaced (the reference is a set of Fortran 90
+ * programs; there is no FFI, the "interface" is the in-process subroutine
+ * sequence of the time loop, cited per entry point below):
+ *   1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90            (C1)
+ *   6_FreeFall_YieldStress/D2Q9_BinghamSediment_Validated_20191127.f90 (C6)
+ *   3_MultiParticle_Sedimentation/D2Q9_RTParticle_20191003.f90 (C3)
+ * A Fortran driver binds these functions through ISO_C_BINDING; a ctypes
+ * binding is used by the Python host layer and the tests.
+ */
+#ifndef LBM2D_H
+#define LBM2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM2D_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    LBM_OK = 0,
+    LBM_E_INVALID = -1,   /* bad argument or parameter value                  */
+    LBM_E_TAU = -2,       /* relaxation time 1/omega < 0.5 (C1:127-130)        */
+    LBM_E_NOMEM = -3,     /* device or host allocation failed                 */
+    LBM_E_CUDA = -4,      /* CUDA runtime error (no device, launch failure)   */
+    LBM_E_NAN = -5,       /* non-finite density or particle state detected    */
+    LBM_E_TIMEOUT = -6,   /* a bounded device-side wait gave up               */
+    LBM_E_OVERFLOW = -7,  /* a lattice tile is touched by too many particles  */
+    LBM_E_STATE = -8,     /* call out of order (e.g. step before particles)   */
+    LBM_E_PARTICLE = -9,  /* particle outside the lattice                     */
+    LBM_E_ABI = -10       /* struct_size does not match this library          */
+};
+
+/* ---- variant switches (compile-time PARAMETERs / IF(0|1) blocks upstream) */
+enum { LBM_FP64 = 0,            /* plain populations in FP64 (drop-in)        */
+       LBM_FP32_SHIFTED = 1 };  /* FP32 storage of f - w_i*rho0, FP32 math    */
+
+enum { LBM_BC_ZOUHE = 0,        /* C1:1250-1258, C1:1341-1363 + corners        */
+       LBM_BC_HALFWAY_BB = 1 }; /* C6:1206-1219, C6:1285-1294 + corners        */
+
+enum { LBM_NEWTONIAN = 0,
+       LBM_BINGHAM = 1 };       /* Papanastasiou-regularised, C6:913-958       */
+
+enum { LBM_RATES_FIXED_Q = 0,   /* C1:1040-1042: s_q given                     */
+       LBM_RATES_Q_OF_OMEGA = 1 /* C6:1009-1011: s_q = 8(2-w)/(8-w)            */ };
+
+enum { LBM_WALL_MIRROR = 0,     /* C1:737-745: mirror-image wall particles     */
+       LBM_WALL_OFFSET = 1,     /* C3:775-783, C6:717-725: wall disk at R out  */
+       LBM_WALL_NONE = 2 };
+
+enum { LBM_CONTACT_DPP = 0,       /* pair contact branch tests D_PP (intent)   */
+       LBM_CONTACT_STALE_DPW = 1  /* tests the stale wall distance D_PW as the
+                                     reference does (C1:721/724, C3:760/763)   */ };
+
+/* ---- parameters -------------------------------------------------------- */
+/* Every constant of MODULE PARAM that the hot path reads is a runtime field
+ * here.  Values that Fortran evaluates as default-kind REAL(4) literals
+ * (PI, 1./36., 1.0/6.0, 1.1, 1.2, 2./9., ...) are passed as the double the
+ * Fortran program actually holds; lbm_params_init() fills them that way. */
+typedef struct lbm_params {
+    int32_t struct_size;      /* must equal sizeof(lbm_params)                 */
+    int32_t nx;               /* NX, C1:8                                      */
+    int32_t ny;               /* NY, C1:9                                      */
+    int32_t precision;        /* LBM_FP64 | LBM_FP32_SHIFTED                   */
+    int32_t bc;               /* LBM_BC_*                                      */
+    int32_t rheology;         /* LBM_NEWTONIAN | LBM_BINGHAM                   */
+    int32_t rate_set;         /* LBM_RATES_*                                   */
+    int32_t wall_model;       /* LBM_WALL_*                                    */
+    int32_t contact_test;     /* LBM_CONTACT_*                                 */
+    int32_t integrate_angle;  /* 1: ANGLE += 0.5(w+w_old) (C6:312)             */
+    int32_t series_every;     /* particle history cadence in steps (>= 1)      */
+    int32_t series_particles; /* particles per history record (<= np)          */
+    int32_t series_capacity;  /* records buffered on the device                */
+    int32_t record_stress;    /* 1: keep stress / yield flag / omega fields    */
+    int32_t device;           /* CUDA device ordinal                           */
+    int32_t reserved0;
+
+    double nu;                /* NU (plastic viscosity Mu_0 for Bingham)       */
+    double rho0;              /* RHO0, C1:57                                   */
+    double s_e, s_eps, s_q;   /* MRT rates omega_e, omega_eps, omega_q         */
+    double d_mrt;             /* d_mrt = 1./36. (C1:881)                       */
+    double inv_six;           /* Inv_Six = 1.0/6.0 (C1:1229)                   */
+    double w_init[3];         /* COMPUTEFEQNEW W0, W1, W2 (C1:1162-1164)       */
+    double pi;                /* PI (C1:3)                                     */
+    double zeta;              /* SPM interface thickness DISK%ZITA (C1:177)    */
+    double gravity;           /* A_G (C1:45): v += (1-rho0/rho_p)*A_G          */
+    double tau_y;             /* TAU_Y                                         */
+    double m_pap;             /* M_PAP, Papanastasiou exponent                 */
+    double gamma_min;         /* zero-shear guard 1.0E-15 (C6:939)             */
+    double rep_zeta;          /* repulsion range ZITA (C1:701)                 */
+    double eps_p, eps_w;      /* EPS_P, EPS_W                                  */
+    double e_p, e_w;          /* E_P, E_W                                      */
+    double c_ij;              /* CIJ = -(RHO_S-RHO_F)*A_G*PI*R^2 (C1:701)      */
+    double wall_mirror_top;   /* 2*WALL%EDGE(3) (C1:741)                       */
+    double wall_mirror_left;  /* 2*WALL%EDGE(4) (C1:743)                       */
+} lbm_params;
+
+/* Particle input record (lbm_set_particles): LBM_PIN doubles per disk. */
+#define LBM_PIN 8   /* x, y, angle, u, v, omega, diam, rho_p */
+
+/* Particle output record (lbm_get_particles): LBM_POUT doubles per disk. */
+#define LBM_POUT 16
+/*  0 x      1 y      2 angle  3 u      4 v      5 omega
+ *  6 Fx     7 Fy     8 Tz        hydrodynamic FORCE(1:3)  (C1:546-570)
+ *  9 Fcol_x 10 Fcol_y            F_COL (C1:596-769)
+ * 11 Fin_x  12 Fin_y  13 Fin_t   F_H_IN (C1:250-252)
+ * 14 mass M_P  15 inertia I_P    (C1:178-179)                              */
+
+/* Field selectors for lbm_get_field. */
+enum {
+    LBM_FIELD_UX = 0,      /* corrected velocity UX (C1:1138-1152)             */
+    LBM_FIELD_UY = 1,
+    LBM_FIELD_RHO = 2,     /* RHO (C1:1421-1439)                               */
+    LBM_FIELD_PHI = 3,     /* total solid fraction sum_p PHI_p (C1:407-484)    */
+    LBM_FIELD_GX = 4,      /* SPM body force G (C1:488-542)                    */
+    LBM_FIELD_GY = 5,
+    LBM_FIELD_TAU11 = 6,   /* STRESS(1:3) of the last collision (C6:947-948)   */
+    LBM_FIELD_TAU22 = 7,
+    LBM_FIELD_TAU12 = 8,
+    LBM_FIELD_OMEGA = 9    /* OMEGA_BN of the last collision (C6:957)          */
+};
+
+/* History record: LBM_SERIES_HEAD + series_particles * LBM_SERIES_PER doubles.
+ * head: step kk, mean density AvgDen (C1:318; NaN when not evaluated)
+ * per particle: x y angle u v omega Fx Fy Tz Fin_x Fin_y Fin_t           */
+#define LBM_SERIES_HEAD 2
+#define LBM_SERIES_PER 12
+
+typedef struct lbm_sim lbm_sim;
+
+/* Fill *p with the constants of C1 as the Fortran program holds them
+ * (REAL(4) literals widened to double), NX/NY = 240/720, FP64, Zou-He. */
+int lbm_params_init(lbm_params* p);
+
+/* Allocate the lattice and initialise it to f = f_eq(rho0, 0) as INITIALIZE
+ * + COMPUTEFEQNEW do (C1:575-592, C1:1157-1175).  Rejects 1/omega < 0.5
+ * with LBM_E_TAU (C1:127-130).  Replaces MAIN's set-up, C1:110-215. */
+int lbm_create(const lbm_params* p, lbm_sim** out);
+int lbm_destroy(lbm_sim* h);
+
+/* Set np disks from np*LBM_PIN doubles; M_P and I_P follow C1:178-179,
+ * VP_OLD and FORCE start at zero as in the reference's static storage.
+ * Replaces the particle read C1:170-179 / C3:145-156 / C6:161-169. */
+int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin);
+
+/* Advance nsteps time steps.  Each step is one pass of the time loop body
+ * C1:241-319 / C6:293-351 / C3:306-399: repulsion, Newton-Euler update,
+ * solid fraction, MRT collision, streaming, boundary conditions,
+ * macroscopic variables, SPM force field, hydrodynamic force, velocity
+ * correction, mean-density check (at history steps). */
+int lbm_step(lbm_sim* h, int32_t nsteps);
+
+/* Completed time steps (KK). */
+int lbm_get_step(lbm_sim* h, int64_t* kk);
+
+/* Copy the particle state (np*LBM_POUT doubles) to host memory. */
+int lbm_get_particles(lbm_sim* h, double* out);
+
+/* Copy one field of (NX+1)*(NY+1) doubles, i fastest (Fortran order of the
+ * reference's (0:NX,0:NY) arrays). */
+int lbm_get_field(lbm_sim* h, int32_t which, double* out);
+
+/* Copy the DOMAIN_IMAGE codes: 10 particle node (some PHI_p >= 0.5,
+ * C1:477-480); for Bingham 5 unyielded / 0 yielded (C6:950-954); else 0. */
+int lbm_get_image(lbm_sim* h, int32_t* out);
+
+/* Drain up to max_records history records into out; *nrec = number copied.
+ * Record length is lbm_series_record_len(h) doubles. */
+int lbm_get_series(lbm_sim* h, double* out, int32_t max_records, int32_t* nrec);
+int lbm_series_record_len(lbm_sim* h, int32_t* len);
+
+/* Mean density SUM(RHO)/((NX+1)(NY+1)) of the current state (C1:318). */
+int lbm_get_mean_density(lbm_sim* h, double* avg);
+
+/* Checkpoint: the complete dynamic state.  f is 9*(NX+1)*(NY+1) doubles in
+ * the reference's F(0:8,0:NX,0:NY) order holding the post-collision
+ * populations of the next step; omega is (NX+1)*(NY+1) doubles (Bingham,
+ * may be NULL otherwise); particles is np*LBM_STATE_PER doubles. */
+#define LBM_STATE_PER 20
+int lbm_get_state(lbm_sim* h, double* f, double* omega, double* particles);
+int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega,
+                  int32_t np, const double* particles);
+
+/* Sticky device status (NaN, overflow, timeout); 0 when healthy. */
+int lbm_get_status(lbm_sim* h);
+
+const char* lbm_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM2D_H */
