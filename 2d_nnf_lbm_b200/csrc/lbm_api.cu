@@ -3,8 +3,8 @@
 //
 // Per time step the host enqueues two kernels on the handle's stream:
 //   k_particles  repulsion, Newton-Euler update, history, tile lists
-//   k_lattice    stream + BC + macro + SPM + force partials + correction +
-//                collision of the next step (last block reduces FORCE)
+//   k_lattice    stream + BC + macro + SPM + force sums + correction +
+//                collision of the next step
 // The post-collision populations live in a ping-pong pair: after step K,
 // f[cur] holds f*(K+1) and f[cur^1] holds f*(K), from which the output
 // kernel re-derives the fields of step K (F after BC, rho, u, G, PHI) on
@@ -41,21 +41,20 @@ struct lbm_sim {
   int np = 0;
   int np_cap = 0;
   double* ps = nullptr;
-  int4* tbox = nullptr;
+  unsigned long long* facc = nullptr;  // [np][6] FORCE accumulators
   int* tile_count = nullptr;
   int* tile_list = nullptr;
+  int* tile_cur = nullptr;
   int tile_cap = MAX_TILE_CAND;
-  int max_slots = 1;
-  double* partials = nullptr;
-  int* cell_count = nullptr;
-  int* cell_start = nullptr;
-  int* cell_items = nullptr;
-  int* cell_of = nullptr;
+  int* nbr = nullptr;
+  int* nbr_count = nullptr;
+  double* nbr_xy = nullptr;
+  int* pair_rebuild = nullptr;
+  bool partials_valid = false;  // facc holds FORCE of the last lattice step
   int ncx = 1, ncy = 1;
   double cell_size = 1.0;
   // scalars
-  unsigned int* ticket = nullptr;
-  double* mass_partials = nullptr;
+  unsigned long long* mass_acc = nullptr;
   long long* d_kk = nullptr;
   double* stale_dpw = nullptr;
   int* h_status = nullptr;  // pinned copy of d_status, refreshed after each call
@@ -72,6 +71,12 @@ struct lbm_sim {
   double* out = nullptr;
   double* out_f = nullptr;
   int64_t out_kk = -1;
+  // per-kernel profiling (lbm_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev;  // 3 per profiled step
+  size_t ev_used = 0;
+  double prof_ms[2] = {0.0, 0.0};
+  int64_t prof_n[2] = {0, 0};
 };
 
 namespace {
@@ -145,21 +150,17 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.om_src = h->om[h->cur];
   a.om_dst = h->om[h->cur ^ 1];
   a.ps = h->ps;
-  a.ps_force = h->ps;
   a.np = h->np;
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
+  a.tile_cur = h->tile_cur;
   a.tile_cap = h->tile_cap;
-  a.tbox = h->tbox;
-  a.partials = h->partials;
-  a.max_slots = h->max_slots;
-  a.ticket = h->ticket;
-  a.mass_partials = h->mass_partials;
+  a.ntiles = h->g.nbx * h->g.nby;
+  a.facc = h->facc;
   a.kk = h->d_kk;
-  a.series = h->series;
+  a.mass_acc = h->series ? h->mass_acc : nullptr;
   a.series_every = h->p.series_every;
   a.series_cap = h->series_cap;
-  a.series_len = h->series_len;
   a.status = h->d_status;
   a.rec = h->rec;
   return a;
@@ -169,11 +170,18 @@ ParticleArgs particle_args(lbm_sim* h) {
   ParticleArgs a{};
   a.ps = h->ps;
   a.np = h->np;
-  a.tbox = h->tbox;
+  a.facc = h->facc;
+  a.decode_force = h->partials_valid ? 1 : 0;
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
+  a.tile_cur = h->tile_cur;
   a.tile_cap = h->tile_cap;
-  a.max_slots = h->max_slots;
+  a.ntiles = h->g.nbx * h->g.nby;
+  a.nbx = h->g.nbx;
+  a.nbr = h->nbr;
+  a.nbr_count = h->nbr_count;
+  a.nbr_xy = h->nbr_xy;
+  a.pair_rebuild = h->pair_rebuild;
   a.wall_model = h->p.wall_model;
   a.contact = h->p.contact_test;
   a.rep_zeta = h->p.rep_zeta;
@@ -187,16 +195,13 @@ ParticleArgs particle_args(lbm_sim* h) {
   a.rho0 = h->p.rho0;
   a.gravity = h->p.gravity;
   a.integrate_angle = h->p.integrate_angle;
-  a.cell_count = h->cell_count;
-  a.cell_start = h->cell_start;
-  a.cell_items = h->cell_items;
-  a.cell_of = h->cell_of;
   a.ncx = h->ncx;
   a.ncy = h->ncy;
   a.cell_size = h->cell_size;
   a.stale_dpw = h->stale_dpw;
   a.kk = h->d_kk;
   a.series = h->series;
+  a.mass_acc = h->series ? h->mass_acc : nullptr;
   a.series_every = h->p.series_every;
   a.series_cap = h->series_cap;
   a.series_len = h->series_len;
@@ -242,11 +247,18 @@ int drain_series(lbm_sim* h) {
   const size_t old = h->host_series.size();
   h->host_series.resize(old + (size_t)(r1 - r0) * len);
   double* dst = h->host_series.data() + old;
+  std::vector<unsigned long long> acc;
   long long r = r0;
+  const double nn = (double)nodes(h);
   while (r < r1) {
     const long long slot = r % h->series_cap;
     long long cnt = std::min<long long>(r1 - r, h->series_cap - slot);
     CK(d2h(h, dst, h->series + slot * len, (size_t)cnt * len * sizeof(double)));
+    acc.resize(cnt);
+    CK(d2h(h, acc.data(), h->mass_acc + slot, (size_t)cnt * sizeof(unsigned long long)));
+    // AvgDen = rho0 + sum(rho - rho0)/N from the fixed-point accumulator
+    for (long long q = 0; q < cnt; ++q)
+      dst[q * len + 1] = h->p.rho0 + (double)(long long)acc[q] / MASS_FIX / nn;
     dst += cnt * len;
     r += cnt;
   }
@@ -272,39 +284,34 @@ int compute_output(lbm_sim* h, bool want_f) {
 
 int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
   // free old
-  dfree(h->ps); dfree(h->tbox); dfree(h->partials);
-  dfree(h->cell_count); dfree(h->cell_start); dfree(h->cell_items); dfree(h->cell_of);
-  dfree(h->series);
-  h->ps = nullptr; h->tbox = nullptr; h->partials = nullptr;
-  h->cell_count = h->cell_start = h->cell_items = h->cell_of = nullptr;
-  h->series = nullptr;
+  dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
+  dfree(h->series); dfree(h->mass_acc);
+  h->ps = nullptr; h->facc = nullptr; h->nbr = nullptr; h->nbr_count = nullptr;
+  h->nbr_xy = nullptr; h->series = nullptr; h->mass_acc = nullptr;
   h->np = np;
-  // tile boxes: radius R + zeta/2 + 1 around the centre
-  const double r = 0.5 * dmax + 0.5 * h->p.zeta + 1.0;
-  const int mtx = (int)std::floor(2.0 * r / TX) + 2;
-  const int mty = (int)std::floor(2.0 * r / TY) + 2;
-  h->max_slots = std::max(1, std::min(mtx, h->g.nbx) * std::min(mty, h->g.nby));
-  h->cell_size = std::max(1.0, dmax + h->p.rep_zeta) * (1.0 + 1e-9);
+  h->partials_valid = false;
+  // pair search cells cover the Verlet radius D_max + repulsion range + SKIN
+  h->cell_size = std::max(1.0, dmax + h->p.rep_zeta + SKIN) * (1.0 + 1e-9);
   h->ncx = std::max(1, (int)std::floor((double)h->p.nx / h->cell_size) + 1);
   h->ncy = std::max(1, (int)std::floor((double)h->p.ny / h->cell_size) + 1);
   int rc;
-  if ((rc = dalloc(&h->ps, (size_t)std::max(np, 1) * PS))) return rc;
-  if ((rc = dalloc(&h->tbox, (size_t)std::max(np, 1)))) return rc;
-  if ((rc = dalloc(&h->partials, (size_t)std::max(np, 1) * h->max_slots * 3))) return rc;
-  const size_t ncells = (size_t)h->ncx * h->ncy;
-  if ((rc = dalloc(&h->cell_count, ncells + 1))) return rc;
-  if ((rc = dalloc(&h->cell_start, ncells + 1))) return rc;
-  if ((rc = dalloc(&h->cell_items, (size_t)std::max(np, 1)))) return rc;
-  if ((rc = dalloc(&h->cell_of, (size_t)std::max(np, 1)))) return rc;
-  CK(cudaMemsetAsync(h->tbox, 0, sizeof(int4) * std::max(np, 1), h->stream));
-  CK(cudaMemsetAsync(h->partials, 0, sizeof(double) * std::max(np, 1) * h->max_slots * 3,
-                     h->stream));
-  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * h->g.nbx * h->g.nby, h->stream));
+  const size_t npa = (size_t)std::max(np, 1);
+  if ((rc = dalloc(&h->ps, npa * PS))) return rc;
+  if ((rc = dalloc(&h->facc, npa * 6))) return rc;
+  if ((rc = dalloc(&h->nbr, npa * MAX_NEIGH))) return rc;
+  if ((rc = dalloc(&h->nbr_count, npa))) return rc;
+  if ((rc = dalloc(&h->nbr_xy, npa * 2))) return rc;
+  CK(cudaMemsetAsync(h->facc, 0, sizeof(unsigned long long) * npa * 6, h->stream));
+  CK(cudaMemsetAsync(h->nbr_count, 0, sizeof(int) * npa, h->stream));
+  CK(cudaMemsetAsync(h->nbr_xy, 0, sizeof(double) * npa * 2, h->stream));
+  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.nbx * h->g.nby, h->stream));
   h->series_np = std::max(0, std::min(h->p.series_particles, np));
   h->series_len = LBM_SERIES_HEAD + LBM_SERIES_PER * h->series_np;
   h->series_cap = std::max(1, h->p.series_capacity);
   if (h->p.series_every > 0) {
     if ((rc = dalloc(&h->series, (size_t)h->series_cap * h->series_len))) return rc;
+    if ((rc = dalloc(&h->mass_acc, (size_t)h->series_cap))) return rc;
+    CK(cudaMemsetAsync(h->mass_acc, 0, sizeof(unsigned long long) * h->series_cap, h->stream));
   }
   return LBM_OK;
 }
@@ -327,7 +334,28 @@ void particle_record(const lbm_params& p, double* P, double x, double y, double 
 
 int launch_tiles(lbm_sim* h) {
   ParticleArgs pa = particle_args(h);
+  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.nbx * h->g.nby, h->stream));
   CK(launch_tiles_only(pa, h->stream));
+  return LBM_OK;
+}
+
+// Particle records with FORCE of the last lattice step: while the
+// accumulators hold it (the next particle kernel decodes them on the
+// device), decode them here the same way.
+int read_particles(lbm_sim* h, std::vector<double>& buf) {
+  buf.assign((size_t)std::max(h->np, 1) * PS, 0.0);
+  CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
+  if (h->partials_valid && h->np > 0) {
+    std::vector<unsigned long long> acc((size_t)h->np * 6);
+    CK(d2h(h, acc.data(), h->facc, acc.size() * sizeof(unsigned long long)));
+    for (int i = 0; i < h->np; ++i) {
+      const unsigned long long* q = &acc[(size_t)i * 6];
+      double* P = &buf[(size_t)i * PS];
+      P[P_FX] = decode_force(q[0], q[1]);
+      P[P_FY] = decode_force(q[2], q[3]);
+      P[P_TZ] = decode_force(q[4], q[5]);
+    }
+  }
   return LBM_OK;
 }
 
@@ -357,16 +385,44 @@ void from_pitched(const std::vector<unsigned char>& buf, double* dst, const lbm_
     for (int i = 0; i < n1x; ++i) dst[(size_t)j * n1x + i] = (double)s[(size_t)j * h->g.pitch + i];
 }
 
+int profile_flush(lbm_sim* h) {
+  if (h->ev_used == 0) return LBM_OK;
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t b = 0; b + 2 < h->ev_used; b += 3) {
+    float t0 = 0.f, t1 = 0.f;
+    CK(cudaEventElapsedTime(&t0, h->ev[b], h->ev[b + 1]));
+    CK(cudaEventElapsedTime(&t1, h->ev[b + 1], h->ev[b + 2]));
+    h->prof_ms[0] += t0;
+    h->prof_ms[1] += t1;
+    h->prof_n[0] += 1;
+    h->prof_n[1] += 1;
+  }
+  h->ev_used = 0;
+  return LBM_OK;
+}
+
+cudaError_t record_event(lbm_sim* h) {
+  if (h->ev_used == h->ev.size()) {
+    cudaEvent_t e;
+    cudaError_t err = cudaEventCreate(&e);
+    if (err != cudaSuccess) return err;
+    h->ev.push_back(e);
+  }
+  return cudaEventRecord(h->ev[h->ev_used++], h->stream);
+}
+
 void destroy_buffers(lbm_sim* h) {
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  h->ev.clear();
   for (int b = 0; b < 2; ++b) {
     dfree(h->f[b]);
     dfree(h->om[b]);
   }
   dfree(h->rec);
-  dfree(h->ps); dfree(h->tbox); dfree(h->partials);
-  dfree(h->cell_count); dfree(h->cell_start); dfree(h->cell_items); dfree(h->cell_of);
-  dfree(h->tile_count); dfree(h->tile_list);
-  dfree(h->ticket); dfree(h->mass_partials); dfree(h->d_kk); dfree(h->stale_dpw);
+  dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
+  dfree(h->tile_count); dfree(h->tile_list); dfree(h->tile_cur); dfree(h->pair_rebuild);
+  dfree(h->mass_acc);
+  dfree(h->d_kk); dfree(h->stale_dpw);
   dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -481,9 +537,25 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   m.m_pap = p.m_pap;
   m.gamma_min = p.gamma_min;
   for (int k = 0; k < 3; ++k) m.w_init[k] = p.w_init[k];
+  // rates at the uniform omega, ComputeRelaxation_MRT (C1:1029-1048, C6:1002-1021)
+  const double oq = m.q_of_omega ? 8. * (2. - omega) / (8. - omega) : p.s_q;
+  const double S_uni[9] = {0.0, p.s_e, p.s_eps, 0.0, oq, 0.0, oq, omega, omega};
+  for (int k = 0; k < 9; ++k) m.S_uni[k] = S_uni[k];
   static const double w[9] = {4.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9, 1.0 / 9,
                               1.0 / 36, 1.0 / 36, 1.0 / 36, 1.0 / 36};
-  for (int k = 0; k < 9; ++k) m.shift_c[k] = p.rho0 * w[k] * (36.0 * p.d_mrt - 1.0);
+  for (int k = 0; k < 9; ++k) m.shift_f[k] = (float)(p.rho0 * w[k] * (36.0 * p.d_mrt - 1.0));
+  m.rho0_f = (float)p.rho0;
+  m.nu_f = (float)p.nu;
+  m.d_mrt_f = (float)p.d_mrt;
+  m.pi_f = (float)p.pi;
+  m.zeta_f = (float)p.zeta;
+  m.tau_y_f = (float)p.tau_y;
+  m.m_pap_f = (float)p.m_pap;
+  m.gamma_min_f = (float)p.gamma_min;
+  m.s_e_f = (float)p.s_e;
+  m.s_eps_f = (float)p.s_eps;
+  m.sq_uni_f = (float)oq;
+  m.omega_f = (float)omega;
 
   int rc = LBM_OK;
   auto fail = [&](int code) {
@@ -509,17 +581,18 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
       cudaMalloc(&h->rec, (size_t)2 * 4 * h->g.plane * h->esz) != cudaSuccess)
     return fail(LBM_E_NOMEM);
   const int ntiles = h->g.nbx * h->g.nby;
-  if ((rc = dalloc(&h->tile_count, ntiles))) return fail(rc);
-  if ((rc = dalloc(&h->tile_list, (size_t)ntiles * h->tile_cap))) return fail(rc);
-  if ((rc = dalloc(&h->ticket, 1))) return fail(rc);
-  if ((rc = dalloc(&h->mass_partials, ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->tile_list, (size_t)2 * ntiles * h->tile_cap))) return fail(rc);
+  if ((rc = dalloc(&h->tile_cur, 1))) return fail(rc);
+  if ((rc = dalloc(&h->pair_rebuild, 1))) return fail(rc);
+  cudaMemsetAsync(h->tile_cur, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(h->pair_rebuild, 0, sizeof(int), h->stream);
   if ((rc = dalloc(&h->d_kk, 1))) return fail(rc);
   if ((rc = dalloc(&h->stale_dpw, 1))) return fail(rc);
   if ((rc = dalloc(&h->out, (size_t)NOUT * nodes(h)))) return fail(rc);
   cudaMemsetAsync(h->f[0], 0, fbytes, h->stream);
   cudaMemsetAsync(h->f[1], 0, fbytes, h->stream);
-  cudaMemsetAsync(h->tile_count, 0, sizeof(int) * ntiles, h->stream);
-  cudaMemsetAsync(h->ticket, 0, sizeof(unsigned int), h->stream);
+  cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * ntiles, h->stream);
   cudaMemsetAsync(h->d_kk, 0, sizeof(long long), h->stream);
   const double inf = INFINITY;
   cudaMemcpyAsync(h->stale_dpw, &inf, sizeof(double), cudaMemcpyHostToDevice, h->stream);
@@ -546,7 +619,7 @@ int lbm_destroy(lbm_sim* h) {
 }
 
 int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
-  if (!h || np < 0 || (np > 0 && !pin)) return LBM_E_INVALID;
+  if (!h || np < 0 || np > MAX_PARTICLES || (np > 0 && !pin)) return LBM_E_INVALID;
   cudaSetDevice(h->p.device);
   double dmax = 0.0;
   for (int i = 0; i < np; ++i) {
@@ -584,13 +657,23 @@ int lbm_step(lbm_sim* h, int32_t nsteps) {
       int rc = drain_series(h);
       if (rc) return rc;
     }
+    if (h->prof) {
+      if (h->ev_used + 3 > 3 * 4096) {
+        int rc = profile_flush(h);
+        if (rc) return rc;
+      }
+      CK(record_event(h));
+    }
     ParticleArgs pa = particle_args(h);
     CK(launch_particles(pa, h->stream));
+    if (h->prof) CK(record_event(h));
+    h->kk += 1;
     LatticeArgs a = lattice_args(h);
     CK(launch_lattice(h, a, 0));
+    if (h->prof) CK(record_event(h));
     h->cur ^= 1;
-    h->kk += 1;
     h->prev_post_bc = false;
+    h->partials_valid = true;
   }
   h->out_kk = -1;
   CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -606,8 +689,9 @@ int lbm_get_step(lbm_sim* h, int64_t* kk) {
 int lbm_get_particles(lbm_sim* h, double* out) {
   if (!h || (!out && h->np > 0)) return LBM_E_INVALID;
   cudaSetDevice(h->p.device);
-  std::vector<double> buf((size_t)std::max(h->np, 1) * PS);
-  CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
+  std::vector<double> buf;
+  int rc = read_particles(h, buf);
+  if (rc) return rc;
   for (int i = 0; i < h->np; ++i) {
     const double* P = &buf[(size_t)i * PS];
     double* r = out + (size_t)LBM_POUT * i;
@@ -742,9 +826,10 @@ int lbm_get_state(lbm_sim* h, double* f, double* omega, double* particles) {
     if (rc) return rc;
   }
   if (particles && h->np > 0) {
-    std::vector<double> buf((size_t)h->np * PS);
+    std::vector<double> buf;
+    int rc = read_particles(h, buf);
+    if (rc) return rc;
     double stale = 0.0;
-    CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
     CK(d2h(h, &stale, h->stale_dpw, sizeof(double)));
     for (int i = 0; i < h->np; ++i) {
       const double* P = &buf[(size_t)i * PS];
@@ -763,7 +848,8 @@ int lbm_get_state(lbm_sim* h, double* f, double* omega, double* particles) {
 
 int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, int32_t np,
                   const double* particles) {
-  if (!h || !f || kk < 0 || np < 0 || (np > 0 && !particles)) return LBM_E_INVALID;
+  if (!h || !f || kk < 0 || np < 0 || np > MAX_PARTICLES || (np > 0 && !particles))
+    return LBM_E_INVALID;
   if (h->m.bingham && !omega) return LBM_E_INVALID;
   cudaSetDevice(h->p.device);
   CK(cudaStreamSynchronize(h->stream));
@@ -820,6 +906,37 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, 
   h->prev_post_bc = true;
   h->out_kk = -1;
   return refreshed_status(h);
+}
+
+int lbm_get_stream(lbm_sim* h, void** stream) {
+  if (!h || !stream) return LBM_E_INVALID;
+  *stream = (void*)h->stream;
+  return LBM_OK;
+}
+
+int lbm_profile(lbm_sim* h, int32_t enable) {
+  if (!h) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  int rc = profile_flush(h);
+  if (rc) return rc;
+  h->prof = enable != 0;
+  h->prof_ms[0] = h->prof_ms[1] = 0.0;
+  h->prof_n[0] = h->prof_n[1] = 0;
+  return LBM_OK;
+}
+
+int lbm_profile_read(lbm_sim* h, double* ms, int64_t* launches) {
+  if (!h || !ms || !launches) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  int rc = profile_flush(h);
+  if (rc) return rc;
+  ms[0] = h->prof_ms[0];
+  ms[1] = h->prof_ms[1];
+  launches[0] = h->prof_n[0];
+  launches[1] = h->prof_n[1];
+  h->prof_ms[0] = h->prof_ms[1] = 0.0;
+  h->prof_n[0] = h->prof_n[1] = 0;
+  return LBM_OK;
 }
 
 int lbm_get_status(lbm_sim* h) {

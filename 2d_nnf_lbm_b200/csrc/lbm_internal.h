@@ -7,8 +7,9 @@
 //                on a 128 B (FP32) / 256 B (FP64) boundary
 //   omega        om[2][NY+1][pitch]     per-node Bingham relaxation rate
 //   particles    ps[np][PS]             one 192 B FP64 record per disk
-//   tile lists   tile_count[ntiles], tile_list[ntiles][tile_cap]
-//   partials     part[np][max_slots][3] per-tile hydrodynamic force sums
+//   force sums   facc[np][6]            exact fixed-point FORCE accumulators
+//   tile lists   tile_count[2][ntiles], tile_list[2][ntiles][tile_cap]
+//   pair lists   nbr_count[np], nbr[np][MAX_NEIGH]  (Verlet lists with skin)
 #pragma once
 
 #include <cstdint>
@@ -20,7 +21,16 @@ namespace lbm {
 constexpr int TX = 32;
 constexpr int TY = 8;
 constexpr int TPB = TX * TY;
-constexpr int MAX_TILE_CAND = 32;  // particles that may touch one tile
+constexpr int MAX_TILE_CAND = 32;   // particles that may touch one tile
+constexpr int MAX_PARTICLES = 4096; // particles per simulation (shared-memory staging)
+constexpr int MAX_NEIGH = 32;       // pair-list entries per particle
+constexpr double SKIN = 2.0;        // Verlet skin (lattice units) of pair and tile lists
+constexpr double MASS_FIX = 1099511627776.0;  // 2^40: fixed-point scale of the mass sum
+// FORCE accumulators: v = hi*2^-20 + lo*2^-62 (both exact integer sums)
+constexpr double FHI = 1048576.0;                  // 2^20
+constexpr double FLO = 4398046511104.0;            // 2^42
+constexpr double FDEC_HI = 1.0 / 1048576.0;        // 2^-20
+constexpr double FDEC_LO = 1.0 / 4611686018427387904.0;  // 2^-62
 
 // Particle record (doubles).
 enum : int {
@@ -30,7 +40,8 @@ enum : int {
   P_FCX, P_FCY,                         // F_COL
   P_FHX, P_FHY, P_FHT,                  // F_H_IN
   P_D, P_RHO, P_M, P_I,                 // DIAM, RHO_P, M_P, I_P
-  P_R0, P_R1, P_R2,
+  P_XT, P_YT,                           // centre at the last tile-list build
+  P_R2,
   PS
 };
 
@@ -57,37 +68,43 @@ struct Model {
   double rho0, nu, omega, s_e, s_eps, s_q, d_mrt, pi, zeta;
   double tau_y, m_pap, gamma_min;
   double w_init[3];
-  double shift_c[9]; // FP32 shifted: rho0*w_k*(36*d_mrt - 1)
+  double S_uni[9];   // rates at the uniform omega (Newtonian nodes)
+  // FP32 copies, so kernels never convert per node
+  float rho0_f, nu_f, d_mrt_f, pi_f, zeta_f, tau_y_f, m_pap_f, gamma_min_f;
+  float s_e_f, s_eps_f, sq_uni_f, omega_f;
+  float shift_f[9];  // rho0*w_k*(36*d_mrt - 1)
 };
 
 struct ParticleArgs {
   double* ps;
   int np;
-  int4* tbox;            // per particle (tx0, ty0, ntx, nty)
-  int* tile_count;
-  int* tile_list;
+  unsigned long long* facc;  // [np][6]
+  int decode_force;          // 1: FORCE = decoded accumulators (then zeroed)
+  int* tile_count;           // [2][ntiles]
+  int* tile_list;            // [2][ntiles][tile_cap]
+  int* tile_cur;             // buffer the lattice kernel reads
   int tile_cap;
-  int max_slots;
+  int ntiles, nbx;
+  int* nbr;                  // [np][MAX_NEIGH]
+  int* nbr_count;            // [np]
+  double* nbr_xy;            // [np][2] centres at the last pair-list build
+  int* pair_rebuild;         // 1: rebuild the pair lists before use
   // repulsion
   int wall_model, contact;
   double rep_zeta, eps_p, eps_w, e_p, e_w, c_ij, mirror_top, mirror_left;
   double rho0, gravity;
   int integrate_angle;
-  // cell list scratch
-  int* cell_count;       // ncells + 1
-  int* cell_start;       // ncells + 1
-  int* cell_items;       // np
-  int* cell_of;          // np
   int ncx, ncy;
   double cell_size;
   double* stale_dpw;
   // bookkeeping
   long long* kk;
   double* series;
+  unsigned long long* mass_acc;  // [series_cap] fixed-point sum of rho - rho0
   int series_every, series_cap, series_len, series_np;
   int* status;
   int nx, ny;
-  double zeta;           // SPM interface thickness (tile box radius)
+  double zeta;               // SPM interface thickness (tile box radius)
 };
 
 struct LatticeArgs {
@@ -98,19 +115,16 @@ struct LatticeArgs {
   const void* om_src;
   void* om_dst;
   const double* ps;
-  double* ps_force;      // same array, written by the last block only
   int np;
-  const int* tile_count;
+  const int* tile_count; // [2][ntiles]
   const int* tile_list;
+  const int* tile_cur;
   int tile_cap;
-  const int4* tbox;
-  double* partials;
-  int max_slots;
-  unsigned int* ticket;
-  double* mass_partials;
+  int ntiles;
+  unsigned long long* facc;
   const long long* kk;
-  double* series;
-  int series_every, series_cap, series_len;
+  unsigned long long* mass_acc;
+  int series_every, series_cap;
   int* status;
   // stress ring: 2 slots x (tau11, tau22, tau12, yield) fields
   void* rec;             // T[2][4][NY+1][pitch]
@@ -133,7 +147,13 @@ cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s);
 
 // Particle kernel (lbm_particles.cu).
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
-// Tile lists only (after set_particles / set_state, before the first step).
+// Tile lists (into buffer 0) and a pair-list rebuild request, after
+// set_particles / set_state.
 cudaError_t launch_tiles_only(const ParticleArgs& a, cudaStream_t s);
+
+// Host and device decode the force accumulators the same way.
+__host__ __device__ inline double decode_force(unsigned long long hi, unsigned long long lo) {
+  return (double)(long long)hi * FDEC_HI + (double)(long long)lo * FDEC_LO;
+}
 
 }  // namespace lbm

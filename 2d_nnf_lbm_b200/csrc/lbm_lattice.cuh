@@ -12,9 +12,9 @@
 //                                                                C6:867-1021
 // and writes f*(k+1).  The collision of step k+1 only reads quantities of
 // step k (rho, corrected u, G, per-node omega), which is why it can run in the
-// same pass as the streaming of step k (C1:292-315 data flow).  The last
-// block to finish reduces the per-tile partials into each particle's FORCE
-// in a fixed order, so results do not depend on block scheduling.
+// same pass as the streaming of step k (C1:292-315 data flow).  Each warp
+// adds its (force, torque) sums into exact fixed-point accumulators per
+// particle, so results do not depend on block scheduling.
 //
 // Precision policies:
 //   double -- plain populations f, operation order of the reference; the TU
@@ -274,7 +274,7 @@ __device__ __forceinline__ void collide_float(const Model& m, float* h, float dr
   float D11 = -dmrt * (t1 + t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gx * ux));
   float D22 = -dmrt * (t1 - t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gy * uy));
   float D12 = -54.0f * dmrt * r.sw * n8 + 0.75f * (-r.sw * (gx * uy + gy * ux));
-  const float NU = (float)m.nu;
+  const float NU = m.nu_f;
   no.t11 = NU * 2.0f * D11;
   no.t22 = NU * 2.0f * D22;
   no.t12 = NU * 2.0f * D12;
@@ -286,12 +286,12 @@ __device__ __forceinline__ void collide_float(const Model& m, float* h, float dr
     D22 *= inv_rho;
     D12 *= inv_rho;
     const float gam = sqrtf(2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12)));
-    const float ty = (float)m.tau_y;
+    const float ty = m.tau_y_f;
     float nua;
-    if (gam < (float)m.gamma_min)
-      nua = NU + (float)m.m_pap * ty;
+    if (gam < m.gamma_min_f)
+      nua = NU + m.m_pap_f * ty;
     else
-      nua = NU + (ty / gam) * (1.0f - expf(-((float)m.m_pap * gam)));
+      nua = NU + (ty / gam) * (1.0f - expf(-(m.m_pap_f * gam)));
     const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
     no.t11 = t11;
     no.t22 = t22;
@@ -378,91 +378,82 @@ __device__ __forceinline__ void pull_interior(const T* __restrict__ src, const G
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic block sum of three doubles (fixed shuffle tree, then warps in
-// order).  All threads of the block must call it.
-__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double (*red)[4],
-                                           int tid) {
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-    c += __shfl_down_sync(0xffffffffu, c, o);
-  }
-  if ((tid & 31) == 0) {
-    red[tid >> 5][0] = a;
-    red[tid >> 5][1] = b;
-    red[tid >> 5][2] = c;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    double sa = 0.0, sb = 0.0, sc = 0.0;
-#pragma unroll
-    for (int w = 0; w < TPB / 32; ++w) {
-      sa += red[w][0];
-      sb += red[w][1];
-      sc += red[w][2];
-    }
-    a = sa;
-    b = sb;
-    c = sc;
-  }
-  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
 }
 
-// ---------------------------------------------------------------------------
+// Exact, order-independent accumulation of a double into two int64 words:
+// v = hi*2^-20 + lo*2^-62 (|v| < 2^43).  Integer sums commute, so the
+// result does not depend on which warp adds first.
+__device__ __forceinline__ void facc_add(unsigned long long* acc, double v) {
+  const double t = v * FHI;
+  const double h = floor(t);
+  const double l = rint((t - h) * FLO);
+  atomicAdd(acc, (unsigned long long)(long long)h);
+  atomicAdd(acc + 1, (unsigned long long)(long long)l);
+}
+
 template <class T, int MODE>
 __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   constexpr bool F64 = sizeof(T) == 8;
-  __shared__ int s_n;
   __shared__ int s_idx[MAX_TILE_CAND];
   __shared__ double s_px[MAX_TILE_CAND], s_py[MAX_TILE_CAND], s_pr[MAX_TILE_CAND];
   __shared__ double s_pu[MAX_TILE_CAND], s_pv[MAX_TILE_CAND], s_pw[MAX_TILE_CAND];
-  __shared__ int4 s_tb[MAX_TILE_CAND];
-  __shared__ double s_red[TPB / 32][4];
-  __shared__ long long s_kk;
-  __shared__ int s_last;
 
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   const int i = blockIdx.x * TX + (tid & (TX - 1));
   const int j = blockIdx.y * TY + tid / TX;
   const int tile = blockIdx.y * a.g.nbx + blockIdx.x;
   const Geometry& g = a.g;
   const Model& m = a.m;
+  (void)warp;
 
-  if (tid == 0) {
-    int c = 0;
-    if (MODE != MODE_INIT) {
-      c = a.tile_count[tile];
-      if (c > a.tile_cap) {
-        atomicOr(a.status, ST_OVERFLOW);
-        c = a.tile_cap;
-      }
-      for (int k = 0; k < c; ++k) {  // ascending particle index: last one wins G
-        const int v = a.tile_list[(long long)tile * a.tile_cap + k];
-        int q = k;
-        while (q > 0 && s_idx[q - 1] > v) {
-          s_idx[q] = s_idx[q - 1];
-          --q;
-        }
-        s_idx[q] = v;
-      }
+  // ---- step number and the particles touching this tile -----------------
+  // Every warp reads the count itself, so tiles without particles never wait
+  // at a barrier; with particles, warp 0 stages them in shared memory sorted
+  // by index (the last particle with PHI>0 sets G, C1:500-507).
+  long long kk = 0;
+  int ncand = 0;
+  if (MODE != MODE_INIT) {
+    long long v = 0;
+    int c = 0, buf = 0;
+    if (lane == 0) {
+      if (MODE == MODE_STEP || MODE == MODE_RESTART) v = *a.kk;
+      buf = *a.tile_cur;
+      c = a.tile_count[(long long)buf * a.ntiles + tile];
     }
-    s_n = c;
-    s_kk = (MODE == MODE_STEP || MODE == MODE_RESTART) ? *a.kk : 0;
+    kk = __shfl_sync(0xffffffffu, v, 0);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    buf = __shfl_sync(0xffffffffu, buf, 0);
+    if (c > a.tile_cap) {
+      if (tid == 0) atomicOr(a.status, ST_OVERFLOW);
+      c = a.tile_cap;
+    }
+    ncand = c;
+    if (ncand > 0) {
+      if (tid < 32) {
+        const long long tbase = (long long)buf * a.ntiles + tile;
+        const int pv = lane < ncand ? a.tile_list[tbase * a.tile_cap + lane] : 0x7fffffff;
+        int rank = 0;
+#pragma unroll 8
+        for (int o = 0; o < 32; ++o) rank += (__shfl_sync(0xffffffffu, pv, o) < pv);
+        if (lane < ncand) {
+          const double* p = a.ps + (long long)pv * PS;
+          s_idx[rank] = pv;
+          s_px[rank] = p[P_X];
+          s_py[rank] = p[P_Y];
+          s_pr[rank] = 0.5 * p[P_D];
+          s_pu[rank] = p[P_U];
+          s_pv[rank] = p[P_V];
+          s_pw[rank] = p[P_W];
+        }
+      }
+      __syncthreads();
+    }
   }
-  __syncthreads();
-  const int ncand = s_n;
-  if (tid < ncand) {
-    const double* p = a.ps + (long long)s_idx[tid] * PS;
-    s_px[tid] = p[P_X];
-    s_py[tid] = p[P_Y];
-    s_pr[tid] = 0.5 * p[P_D];
-    s_pu[tid] = p[P_U];
-    s_pv[tid] = p[P_V];
-    s_pw[tid] = p[P_W];
-    s_tb[tid] = a.tbox[s_idx[tid]];
-  }
-  __syncthreads();
 
   const bool act = (i <= g.nx) && (j <= g.ny);
   const long long n = (long long)j * g.pitch + i;
@@ -497,70 +488,71 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   // ---- macroscopic variables (C1:1421-1439) ----------------------------
   T rho, drho, ux, uy;
   if (initial) {
-    rho = (T)m.rho0;
+    rho = F64 ? (T)m.rho0 : (T)m.rho0_f;
     drho = (T)0;
     ux = (T)0;
     uy = (T)0;
   } else if (F64) {
     rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-    drho = rho;
+    drho = rho - (T)m.rho0;
     const T rinv = (T)1.0 / rho;
     ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
     uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
   } else {
     drho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
-    rho = (T)m.rho0 + drho;
-    const T rinv = (T)1.0 / rho;
+    rho = (T)m.rho0_f + drho;
+    const T rinv = (T)__frcp_rn((float)rho);
     ux = rinv * ((f[1] + f[5] + f[8]) - (f[6] + f[3] + f[7]));
     uy = rinv * ((f[5] + f[2] + f[6]) - (f[7] + f[4] + f[8]));
   }
   if (!act) {
     rho = (T)1;
+    drho = (T)0;
     ux = uy = (T)0;
   }
 
-  // ---- SPM: G (last particle with PHI>0 wins) and force partials --------
+  // ---- SPM: G (last particle with PHI>0 wins) and the hydrodynamic force -
   T gx = (T)0, gy = (T)0;
   double phisum = 0.0;
   bool pnode = false;
-  if (MODE != MODE_INIT) {
-    for (int c = 0; c < ncand; ++c) {
-      double fx = 0.0, fy = 0.0, tz = 0.0;
-      if (act) {
-        const double di = (double)i - s_px[c];
-        const double dj = (double)j - s_py[c];
-        T phi;
-        if (F64)
-          phi = (T)phi_double(di, dj, s_pr[c], m.zeta, m.pi);
-        else
-          phi = (T)phi_float((float)di, (float)dj, (float)s_pr[c], (float)m.zeta, (float)m.pi);
-        if (phi > (T)0) {
-          const T uxp = (T)s_pu[c] - (T)s_pw[c] * (T)dj;
-          const T uyp = (T)s_pv[c] + (T)s_pw[c] * (T)di;
-          if (!initial) {
-            gx = phi * (uxp - ux);
-            gy = phi * (uyp - uy);
-          }
-          if (MODE == MODE_STEP) {
-            const T rp = rho * phi;
-            fx = (double)(rp * (ux - uxp));
-            fy = (double)(rp * (uy - uyp));
-            tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
-          }
-          phisum += (double)phi;
-          if (phi >= (T)0.5) pnode = true;
+  for (int c = 0; c < ncand; ++c) {
+    double fx = 0.0, fy = 0.0, tz = 0.0;
+    bool hit = false;
+    if (act) {
+      const double di = (double)i - s_px[c];
+      const double dj = (double)j - s_py[c];
+      T phi;
+      if (F64)
+        phi = (T)phi_double(di, dj, s_pr[c], m.zeta, m.pi);
+      else
+        phi = (T)phi_float((float)di, (float)dj, (float)s_pr[c], m.zeta_f, m.pi_f);
+      if (phi > (T)0) {
+        hit = true;
+        const T uxp = (T)s_pu[c] - (T)s_pw[c] * (T)dj;
+        const T uyp = (T)s_pv[c] + (T)s_pw[c] * (T)di;
+        if (!initial) {
+          gx = phi * (uxp - ux);
+          gy = phi * (uyp - uy);
         }
+        if (MODE == MODE_STEP) {
+          const T rp = rho * phi;
+          fx = (double)(rp * (ux - uxp));
+          fy = (double)(rp * (uy - uyp));
+          tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
+        }
+        phisum += (double)phi;
+        if (phi >= (T)0.5) pnode = true;
       }
-      if (MODE == MODE_STEP) {
-        block_sum3(fx, fy, tz, s_red, tid);
-        if (tid == 0) {
-          const int4 tb = s_tb[c];
-          const int slot = (blockIdx.y - tb.y) * tb.z + (blockIdx.x - tb.x);
-          double* dstp = a.partials + ((long long)s_idx[c] * a.max_slots + slot) * 3;
-          dstp[0] = fx;
-          dstp[1] = fy;
-          dstp[2] = tz;
-        }
+    }
+    if (MODE == MODE_STEP && __any_sync(0xffffffffu, hit)) {
+      fx = warp_sum(fx);
+      fy = warp_sum(fy);
+      tz = warp_sum(tz);
+      if (lane == 0) {
+        unsigned long long* acc = a.facc + (long long)s_idx[c] * 6;
+        facc_add(acc, fx);
+        facc_add(acc + 2, fy);
+        facc_add(acc + 4, tz);
       }
     }
   }
@@ -589,106 +581,72 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
     return;
   }
 
+  // ---- mean density at history steps (C1:318): fixed-point, order-free ---
+  if (MODE == MODE_STEP && a.series_every > 0 && a.mass_acc != nullptr &&
+      (kk % a.series_every) == 0) {
+    double s0 = warp_sum((double)drho);
+    if (lane == 0) {
+      const long long slot = (kk / a.series_every - 1) % a.series_cap;
+      const long long q = __double2ll_rn(s0 * MASS_FIX);
+      atomicAdd(a.mass_acc + slot, (unsigned long long)q);
+    }
+  }
+
   // ---- collision of the next step ---------------------------------------
+  if (!act) return;
   NodeOut no;
   no.omega = m.omega;
   no.yield = 0;
   no.t11 = no.t22 = no.t12 = 0.0;
   const bool want_stress = m.bingham || m.record_stress;
-  if (act) {
-    double omega_node = m.omega;
-    if (m.bingham && MODE != MODE_INIT) omega_node = (double)static_cast<const T*>(a.om_src)[n];
-    if (F64) {
-      double S[9];
-      rates_double(m, omega_node, S);
-      double fd[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) fd[k] = (double)f[k];
-      collide_double(m, fd, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, S,
-                     want_stress, no);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = (T)fd[k];
+  const bool node_omega = m.bingham && MODE != MODE_INIT;
+  if (F64) {
+    double S[9];
+    if (node_omega) {
+      rates_double(m, (double)static_cast<const T*>(a.om_src)[n], S);
     } else {
-      Rates32 r;
-      r.s1 = (float)m.s_e;
-      r.s2 = (float)m.s_eps;
-      const float w = (float)omega_node;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) S[k] = m.S_uni[k];
+    }
+    double fd[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fd[k] = (double)f[k];
+    collide_double(m, fd, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, S,
+                   want_stress, no);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (T)fd[k];
+  } else {
+    Rates32 r;
+    r.s1 = m.s_e_f;
+    r.s2 = m.s_eps_f;
+    if (node_omega) {
+      const float w = (float)static_cast<const T*>(a.om_src)[n];
       r.sw = w;
-      r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : (float)m.s_q;
-      float sh[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) sh[k] = (float)m.shift_c[k];
-      float hf[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) hf[k] = (float)f[k];
-      collide_float(m, hf, (float)drho, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy,
-                    r, (float)m.d_mrt, sh, want_stress, no);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
+      r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : m.sq_uni_f;
+    } else {
+      r.sw = m.omega_f;
+      r.sq = m.sq_uni_f;
     }
-    T* __restrict__ dst = static_cast<T*>(a.dst);
+    float hf[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) dst[k * g.plane + n] = f[k];
-    if (m.bingham) static_cast<T*>(a.om_dst)[n] = (T)no.omega;
-    if (m.record_stress) {
-      const int slot = (int)((s_kk + 1) & 1);
-      T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * g.plane;
-      rec[n] = (T)no.t11;
-      rec[g.plane + n] = (T)no.t22;
-      rec[2 * g.plane + n] = (T)no.t12;
-      rec[3 * g.plane + n] = (T)no.yield;
-    }
+    for (int k = 0; k < 9; ++k) hf[k] = (float)f[k];
+    collide_float(m, hf, (float)drho, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy,
+                  r, m.d_mrt_f, m.shift_f, want_stress, no);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
   }
-  if (MODE != MODE_STEP) return;
-
-  // ---- mean density at history steps (C1:318) ----------------------------
-  const long long kk = s_kk;
-  const bool rec_step = a.series_every > 0 && (kk % a.series_every) == 0 && a.series != nullptr;
-  const int nblocks = gridDim.x * gridDim.y;
-  if (rec_step) {
-    double s0 = act ? (F64 ? (double)rho : (double)drho) : 0.0, s1 = 0.0, s2 = 0.0;
-    block_sum3(s0, s1, s2, s_red, tid);
-    if (tid == 0) a.mass_partials[tile] = s0;
+  T* __restrict__ dst = static_cast<T*>(a.dst);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) dst[k * g.plane + n] = f[k];
+  if (m.bingham) static_cast<T*>(a.om_dst)[n] = (T)no.omega;
+  if (m.record_stress) {
+    const int slot = (int)((kk + 1) & 1);
+    T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * g.plane;
+    rec[n] = (T)no.t11;
+    rec[g.plane + n] = (T)no.t22;
+    rec[2 * g.plane + n] = (T)no.t12;
+    rec[3 * g.plane + n] = (T)no.yield;
   }
-
-  // ---- last block: fixed-order reduction of FORCE and mass ---------------
-  if (tid == 0) {
-    __threadfence();
-    const unsigned int t = atomicAdd(a.ticket, 1u);
-    s_last = (t == (unsigned int)(nblocks - 1));
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  for (int p = tid; p < a.np; p += TPB) {
-    const int4 tb = a.tbox[p];
-    const double* pp = a.partials + (long long)p * a.max_slots * 3;
-    double fx = 0.0, fy = 0.0, tz = 0.0;
-    const int ns = tb.z * tb.w;
-    for (int s = 0; s < ns; ++s) {
-      fx += __ldcg(pp + 3 * s);
-      fy += __ldcg(pp + 3 * s + 1);
-      tz += __ldcg(pp + 3 * s + 2);
-    }
-    double* q = a.ps_force + (long long)p * PS;
-    q[P_FX] = fx;
-    q[P_FY] = fy;
-    q[P_TZ] = tz;
-    if (!isfinite(fx) || !isfinite(fy) || !isfinite(tz)) atomicOr(a.status, ST_NAN);
-  }
-  if (rec_step) {
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int b = tid; b < nblocks; b += TPB) s0 += __ldcg(a.mass_partials + b);
-    block_sum3(s0, s1, s2, s_red, tid);
-    if (tid == 0) {
-      const double nn = (double)((long long)(g.nx + 1) * (g.ny + 1));
-      const double avg = F64 ? s0 / nn : m.rho0 + s0 / nn;
-      const long long r = (kk / a.series_every - 1) % a.series_cap;
-      a.series[r * a.series_len + 1] = avg;
-      if (!isfinite(avg)) atomicOr(a.status, ST_NAN);
-    }
-  }
-  if (tid == 0) *a.ticket = 0u;
 }
 
 template <class T>

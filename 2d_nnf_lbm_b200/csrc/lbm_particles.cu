@@ -1,15 +1,19 @@
 // lbm_particles.cu -- particle kernel of one time step (sm_100a).
 //
-// One block of PBLK threads, particles strided over the threads:
-//   1. cell list of disk centres (counting sort into cells of edge
-//      >= D_max + repulsion range), so each disk only tests the disks of its
-//      3x3 neighbour cells;
+// One block of PBLK threads; the particle centres and diameters are staged in
+// shared memory:
+//   0. FORCE of the previous lattice step, decoded from the exact fixed-point
+//      accumulators the lattice kernel filled (ComputeForce_HYDRO, C1:546-570);
+//   1. Verlet pair lists (cut-off + SKIN) rebuilt from a hashed cell grid only
+//      when some disk moved more than SKIN/2 since the last build;
 //   2. Glowinski repulsion, pairs then walls (C1:701-768, C3:739-804); each
-//      disk sums its pair forces in ascending partner order, which is the
-//      order in which the reference's IP<JP double loop accumulates them;
-//   3. Newton-Euler update with the internal-mass term (C1:247-259,
+//      disk sums its pair forces in ascending partner order, the order in
+//      which the reference's IP<JP double loop accumulates them;
+//      Newton-Euler update with the internal-mass term (C1:247-259,
 //      C6:300-312) and the history record (C1:264, C6:315-318);
-//   4. per-tile candidate lists for the lattice kernel's SPM evaluation.
+//   3. per-tile candidate lists for the lattice kernel's SPM evaluation,
+//      rebuilt (radius R + zeta/2 + 1 + SKIN) into the idle buffer only when
+//      some disk moved more than SKIN/2 from where the lists were built.
 // Built with --fmad=false: the FP64 arithmetic is operation-for-operation the
 // reference's, so the particle update is bit-identical for identical inputs.
 #include <cuda_runtime.h>
@@ -18,31 +22,35 @@
 
 namespace lbm {
 
-constexpr int PBLK = 256;
-constexpr int MAX_NEIGH = 32;
+constexpr int PBLK = 1024;
+constexpr int HASH = 4096;  // power of two
+
+struct PShared {
+  int cnt[HASH + 1];
+  int start[HASH + 1];
+  int items[MAX_PARTICLES];
+  int key[MAX_PARTICLES];
+  double x[MAX_PARTICLES], y[MAX_PARTICLES], d[MAX_PARTICLES];
+  int scan[PBLK / 32];
+};
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
-
-__device__ __forceinline__ int cell_index(const ParticleArgs& a, double x, double y) {
-  const int cx = clampi((int)floor(x / a.cell_size), 0, a.ncx - 1);
-  const int cy = clampi((int)floor(y / a.cell_size), 0, a.ncy - 1);
-  return cy * a.ncx + cx;
-}
 
 // Pair force of (lo, hi), lo < hi, as the reference evaluates F_PP for
 // IP = lo, JP = hi (C3:758-766); the contact branch tests D_PP or the stale
 // wall distance D_PW.
-__device__ __forceinline__ void pair_force(const ParticleArgs& a, const double* A, const double* B,
-                                           double test_stale, double* F) {
+__device__ __forceinline__ void pair_force(const ParticleArgs& a, double ax, double ay, double ad,
+                                           double bx, double by, double bd, double test_stale,
+                                           double* F) {
   const double ZITA = a.rep_zeta, CIJ = a.c_ij, EPS_P = a.eps_p, E_P = a.e_p;
-  const double dx = A[P_X] - B[P_X], dy = A[P_Y] - B[P_Y];
+  const double dx = ax - bx, dy = ay - by;
   const double D_PP = sqrt(dx * dx + dy * dy);
-  const double rsum = 0.5 * A[P_D] + 0.5 * B[P_D];
+  const double rsum = 0.5 * ad + 0.5 * bd;
   const double test = a.contact == 1 ? test_stale : D_PP;
   F[0] = 0.0;
   F[1] = 0.0;
   if (D_PP > rsum + ZITA) return;
-  const double q = (D_PP - 0.5 * A[P_D] - 0.5 * B[P_D] - ZITA) / ZITA;
+  const double q = (D_PP - 0.5 * ad - 0.5 * bd - ZITA) / ZITA;
   if (D_PP <= rsum + ZITA && test > rsum) {
     F[0] = EPS_P * CIJ * (q * q) * dx / D_PP;
     F[1] = EPS_P * CIJ * (q * q) * dy / D_PP;
@@ -53,152 +61,208 @@ __device__ __forceinline__ void pair_force(const ParticleArgs& a, const double* 
   }
 }
 
-__device__ void build_tiles(const ParticleArgs& a, int tid) {
-  // clear the tiles of the previous boxes
-  for (int p = tid; p < a.np; p += PBLK) {
-    const int4 tb = a.tbox[p];
-    for (int ty = 0; ty < tb.w; ++ty)
-      for (int tx = 0; tx < tb.z; ++tx) {
-        const int nbx = (a.nx + 1 + TX - 1) / TX;
-        a.tile_count[(tb.y + ty) * nbx + tb.x + tx] = 0;
-      }
-  }
-  __syncthreads();
-  const int nbx = (a.nx + 1 + TX - 1) / TX;
-  for (int p = tid; p < a.np; p += PBLK) {
-    const double* P = a.ps + (long long)p * PS;
-    const double r = 0.5 * P[P_D] + 0.5 * a.zeta + 1.0;
-    int i0 = (int)ceil(P[P_X] - r), i1 = (int)floor(P[P_X] + r);
-    int j0 = (int)ceil(P[P_Y] - r), j1 = (int)floor(P[P_Y] + r);
-    i0 = max(i0, 0);
-    j0 = max(j0, 0);
-    i1 = min(i1, a.nx);
-    j1 = min(j1, a.ny);
-    int4 tb = make_int4(0, 0, 0, 0);
-    if (i0 <= i1 && j0 <= j1 && isfinite(P[P_X]) && isfinite(P[P_Y])) {
-      tb.x = i0 / TX;
-      tb.y = j0 / TY;
-      tb.z = i1 / TX - tb.x + 1;
-      tb.w = j1 / TY - tb.y + 1;
-      if (tb.z * tb.w > a.max_slots) {
-        atomicOr(a.status, ST_OVERFLOW);
-        tb = make_int4(0, 0, 0, 0);
+// Insert disk p into the candidate lists of the tiles within R + zeta/2 + 1
+// + SKIN of (x, y); atomics are issued four at a time so latencies overlap.
+__device__ __forceinline__ void insert_tiles(const ParticleArgs& a, int p, double x, double y,
+                                             double D, int buf) {
+  const double r = 0.5 * D + 0.5 * a.zeta + 1.0 + SKIN;
+  int i0 = max((int)ceil(x - r), 0), i1 = min((int)floor(x + r), a.nx);
+  int j0 = max((int)ceil(y - r), 0), j1 = min((int)floor(y + r), a.ny);
+  if (!(i0 <= i1 && j0 <= j1) || !isfinite(x) || !isfinite(y)) return;
+  const int tx0 = i0 / TX, ty0 = j0 / TY, ntx = i1 / TX - tx0 + 1, nty = j1 / TY - ty0 + 1;
+  int* cnt = a.tile_count + (long long)buf * a.ntiles;
+  int* lst = a.tile_list + (long long)buf * a.ntiles * a.tile_cap;
+  const int nt = ntx * nty;
+  for (int t0 = 0; t0 < nt; t0 += 4) {
+    int tt[4], sl[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u;
+      tt[u] = -1;
+      if (t < nt) {
+        const int ty = t / ntx, tx = t - ty * ntx;
+        tt[u] = (ty0 + ty) * a.nbx + tx0 + tx;
+        sl[u] = atomicAdd(&cnt[tt[u]], 1);
       }
     }
-    for (int ty = 0; ty < tb.w; ++ty)
-      for (int tx = 0; tx < tb.z; ++tx) {
-        const int t = (tb.y + ty) * nbx + tb.x + tx;
-        const int slot = atomicAdd(&a.tile_count[t], 1);
-        if (slot < a.tile_cap)
-          a.tile_list[(long long)t * a.tile_cap + slot] = p;
-        else
-          atomicOr(a.status, ST_OVERFLOW);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (tt[u] < 0) continue;
+      if (sl[u] < a.tile_cap)
+        lst[(long long)tt[u] * a.tile_cap + sl[u]] = p;
+      else
+        atomicOr(a.status, ST_OVERFLOW);
+    }
+  }
+}
+
+__device__ __forceinline__ int cell_key(const ParticleArgs& a, double x, double y) {
+  const int cx = clampi((int)floor(x / a.cell_size), 0, a.ncx - 1);
+  const int cy = clampi((int)floor(y / a.cell_size), 0, a.ncy - 1);
+  return cy * a.ncx + cx;
+}
+
+// Verlet lists: hash the staged centres into HASH buckets (counting sort),
+// then collect, for each disk, the partners within cut-off + SKIN in
+// ascending index order.
+__device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int b = tid; b <= HASH; b += PBLK) S.cnt[b] = 0;
+  __syncthreads();
+  for (int p = tid; p < a.np; p += PBLK) {
+    const int key = cell_key(a, S.x[p], S.y[p]);
+    S.key[p] = key;
+    atomicAdd(&S.cnt[key & (HASH - 1)], 1);
+  }
+  __syncthreads();
+  constexpr int PER = HASH / PBLK;
+  int loc[PER];
+  int sum = 0;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    loc[u] = S.cnt[tid * PER + u];
+    sum += loc[u];
+  }
+  int incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) S.scan[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = lane < PBLK / 32 ? S.scan[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += v;
+    }
+    if (lane < PBLK / 32) S.scan[lane] = wi - w;
+  }
+  __syncthreads();
+  int run = S.scan[warp] + incl - sum;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    S.start[tid * PER + u] = run;
+    S.cnt[tid * PER + u] = run;  // scatter cursor
+    run += loc[u];
+  }
+  if (tid == PBLK - 1) S.start[HASH] = run;
+  __syncthreads();
+  for (int p = tid; p < a.np; p += PBLK) {
+    const int slot = atomicAdd(&S.cnt[S.key[p] & (HASH - 1)], 1);
+    S.items[slot] = p;
+  }
+  __syncthreads();
+  for (int p = tid; p < a.np; p += PBLK) {
+    const double px = S.x[p], py = S.y[p], pd = S.d[p];
+    int* nb = a.nbr + (long long)p * MAX_NEIGH;
+    int nn = 0;
+    const int key = S.key[p];
+    const int cx = key % a.ncx, cy = key / a.ncx;
+    for (int yy = max(cy - 1, 0); yy <= min(cy + 1, a.ncy - 1); ++yy)
+      for (int xx = max(cx - 1, 0); xx <= min(cx + 1, a.ncx - 1); ++xx) {
+        const int ck = yy * a.ncx + xx;
+        const int b = ck & (HASH - 1);
+        for (int s = S.start[b]; s < S.start[b + 1]; ++s) {
+          const int q = S.items[s];
+          if (q == p || S.key[q] != ck) continue;
+          const double dx = px - S.x[q], dy = py - S.y[q];
+          const double lim = 0.5 * pd + 0.5 * S.d[q] + a.rep_zeta + SKIN;
+          if (dx * dx + dy * dy > lim * lim) continue;
+          if (nn < MAX_NEIGH) {
+            int k = nn++;
+            while (k > 0 && nb[k - 1] > q) {
+              nb[k] = nb[k - 1];
+              --k;
+            }
+            nb[k] = q;
+          } else {
+            atomicOr(a.status, ST_OVERFLOW);
+          }
+        }
       }
-    a.tbox[p] = tb;
+    a.nbr_count[p] = nn;
+    a.nbr_xy[2 * p] = px;
+    a.nbr_xy[2 * p + 1] = py;
   }
 }
 
 __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PShared& S = *reinterpret_cast<PShared*>(smem_raw);
   __shared__ long long s_kk;
-  __shared__ int s_sum[PBLK];
+  __shared__ int s_pairs, s_tiles;
   const int tid = threadIdx.x;
+
   if (tid == 0) {
     s_kk = *a.kk + 1;
     *a.kk = s_kk;
-  }
-  __syncthreads();
-  const long long kk = s_kk;
-
-  // ---- 1. cell list ------------------------------------------------------
-  const int ncells = a.ncx * a.ncy;
-  if (a.np > 1) {
-    for (int c = tid; c < ncells; c += PBLK) a.cell_count[c] = 0;
-    __syncthreads();
-    for (int p = tid; p < a.np; p += PBLK) {
-      const double* P = a.ps + (long long)p * PS;
-      const int c = cell_index(a, P[P_X], P[P_Y]);
-      a.cell_of[p] = c;
-      atomicAdd(&a.cell_count[c], 1);
-    }
-    __syncthreads();
-    const int chunk = (ncells + PBLK - 1) / PBLK;
-    const int c0 = tid * chunk, c1 = min(ncells, c0 + chunk);
-    int local = 0;
-    for (int c = c0; c < c1; ++c) local += a.cell_count[c];
-    s_sum[tid] = local;
-    __syncthreads();
-    if (tid == 0) {
-      int run = 0;
-      for (int t = 0; t < PBLK; ++t) {
-        const int v = s_sum[t];
-        s_sum[t] = run;
-        run += v;
-      }
-    }
-    __syncthreads();
-    int run = s_sum[tid];
-    for (int c = c0; c < c1; ++c) {
-      const int v = a.cell_count[c];
-      a.cell_start[c] = run;
-      a.cell_count[c] = run;  // becomes the scatter cursor
-      run += v;
-    }
-    if (tid == 0) a.cell_start[ncells] = a.np;
-    __syncthreads();
-    for (int p = tid; p < a.np; p += PBLK) {
-      const int slot = atomicAdd(&a.cell_count[a.cell_of[p]], 1);
-      a.cell_items[slot] = p;
-    }
+    s_pairs = *a.pair_rebuild;
+    s_tiles = 0;
   }
   const double stale = *a.stale_dpw;  // D_PW left over from the previous call
   __syncthreads();
-
-  // ---- 2./3. repulsion, Newton-Euler update, history ----------------------
+  const long long kk = s_kk;
   const bool rec = a.series != nullptr && a.series_every > 0 && (kk % a.series_every) == 0;
   const long long rslot = rec ? (kk / a.series_every - 1) % a.series_cap : 0;
   if (rec && tid == 0) {
     a.series[rslot * a.series_len + 0] = (double)kk;
     a.series[rslot * a.series_len + 1] = __longlong_as_double(0x7ff8000000000000LL);
+    if (a.mass_acc) a.mass_acc[rslot] = 0ull;
   }
+
+  // ---- 0. FORCE of the last lattice step; stage centres ------------------
   for (int p = tid; p < a.np; p += PBLK) {
     double* P = a.ps + (long long)p * PS;
+    if (a.decode_force) {
+      unsigned long long* acc = a.facc + (long long)p * 6;
+      const double fx = decode_force(acc[0], acc[1]);
+      const double fy = decode_force(acc[2], acc[3]);
+      const double tz = decode_force(acc[4], acc[5]);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) acc[k] = 0ull;
+      P[P_FX] = fx;
+      P[P_FY] = fy;
+      P[P_TZ] = tz;
+      if (!isfinite(fx) || !isfinite(fy) || !isfinite(tz)) atomicOr(a.status, ST_NAN);
+    }
+    const double x = P[P_X], y = P[P_Y];
+    S.x[p] = x;
+    S.y[p] = y;
+    S.d[p] = P[P_D];
+    if (a.np > 1) {
+      const double ddx = x - a.nbr_xy[2 * p], ddy = y - a.nbr_xy[2 * p + 1];
+      if (!(ddx * ddx + ddy * ddy <= 0.25 * SKIN * SKIN)) s_pairs = 1;
+    }
+  }
+  __syncthreads();
+
+  // ---- 1. pair lists -------------------------------------------------------
+  if (a.np > 1 && s_pairs) {
+    rebuild_pairs(a, S);
+    if (tid == 0) *a.pair_rebuild = 0;
+  }
+
+  // ---- 2. repulsion, Newton-Euler update, history -------------------------
+  for (int p = tid; p < a.np; p += PBLK) {
+    double* P = a.ps + (long long)p * PS;
+    const double px = S.x[p], py = S.y[p], pd = S.d[p];
     double fcx = 0.0, fcy = 0.0;
     if (a.np > 1) {
-      int nb[MAX_NEIGH];
-      int nn = 0;
-      const int c = a.cell_of[p];
-      const int cx = c % a.ncx, cy = c / a.ncx;
-      for (int yy = max(cy - 1, 0); yy <= min(cy + 1, a.ncy - 1); ++yy)
-        for (int xx = max(cx - 1, 0); xx <= min(cx + 1, a.ncx - 1); ++xx) {
-          const int cc = yy * a.ncx + xx;
-          for (int s = a.cell_start[cc]; s < a.cell_start[cc + 1]; ++s) {
-            const int q = a.cell_items[s];
-            if (q == p) continue;
-            const double* Q = a.ps + (long long)q * PS;
-            const double dx = P[P_X] - Q[P_X], dy = P[P_Y] - Q[P_Y];
-            const double lim = 0.5 * P[P_D] + 0.5 * Q[P_D] + a.rep_zeta;
-            if (dx * dx + dy * dy > 1.0000001 * lim * lim + 1e-12) continue;
-            if (nn < MAX_NEIGH) {
-              int k = nn++;
-              while (k > 0 && nb[k - 1] > q) {
-                nb[k] = nb[k - 1];
-                --k;
-              }
-              nb[k] = q;
-            } else {
-              atomicOr(a.status, ST_OVERFLOW);
-            }
-          }
-        }
+      const int* nb = a.nbr + (long long)p * MAX_NEIGH;
+      const int nn = a.nbr_count[p];
       for (int k = 0; k < nn; ++k) {
         const int q = nb[k];
         double F[2];
         if (q < p) {
-          pair_force(a, a.ps + (long long)q * PS, P, stale, F);
+          pair_force(a, S.x[q], S.y[q], S.d[q], px, py, pd, stale, F);
           fcx = fcx - F[0];
           fcy = fcy - F[1];
         } else {
-          pair_force(a, P, a.ps + (long long)q * PS, stale, F);
+          pair_force(a, px, py, pd, S.x[q], S.y[q], S.d[q], stale, F);
           fcx = fcx + F[0];
           fcy = fcy + F[1];
         }
@@ -207,7 +271,7 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     // walls (C1:735-768 mirror images; C3:775-804 wall disks)
     if (a.wall_model != 2) {
       const double ZITA = a.rep_zeta, CIJ = a.c_ij, EPS_W = a.eps_w, E_W = a.e_w;
-      const double x = P[P_X], y = P[P_Y], D = P[P_D];
+      const double x = px, y = py, D = pd;
       double D_PW = stale;
       for (int iw = 1; iw <= 4; ++iw) {
         double rw0, rw1;
@@ -248,54 +312,93 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     const double RHO0 = a.rho0;
     const double rr = RHO0 / P[P_RHO];
     const double M = P[P_M], I = P[P_I];
-    const double fh0 = rr * M * (P[P_U] - P[P_UO]);
-    const double fh1 = rr * M * (P[P_V] - P[P_VO]);
-    const double fh2 = rr * I * (P[P_W] - P[P_WO]);
-    const double vo0 = P[P_U], vo1 = P[P_V], vo2 = P[P_W];
-    const double v0 = P[P_U] + P[P_FX] / M + fh0 / M + fcx / M;
-    const double v1 = P[P_V] + P[P_FY] / M + fh1 / M + (1.0 - RHO0 / P[P_RHO]) * a.gravity + fcy / M;
-    const double v2 = P[P_W] + P[P_TZ] / I + fh2 / I;
+    const double u0 = P[P_U], u1 = P[P_V], u2 = P[P_W];
+    const double fh0 = rr * M * (u0 - P[P_UO]);
+    const double fh1 = rr * M * (u1 - P[P_VO]);
+    const double fh2 = rr * I * (u2 - P[P_WO]);
+    const double v0 = u0 + P[P_FX] / M + fh0 / M + fcx / M;
+    const double v1 = u1 + P[P_FY] / M + fh1 / M + (1.0 - RHO0 / P[P_RHO]) * a.gravity + fcy / M;
+    const double v2 = u2 + P[P_TZ] / I + fh2 / I;
+    const double nx_ = px + 0.5 * (v0 + u0);
+    const double ny_ = py + 0.5 * (v1 + u1);
     P[P_FHX] = fh0;
     P[P_FHY] = fh1;
     P[P_FHT] = fh2;
-    P[P_UO] = vo0;
-    P[P_VO] = vo1;
-    P[P_WO] = vo2;
+    P[P_UO] = u0;
+    P[P_VO] = u1;
+    P[P_WO] = u2;
     P[P_U] = v0;
     P[P_V] = v1;
     P[P_W] = v2;
-    P[P_X] = P[P_X] + 0.5 * (v0 + vo0);
-    P[P_Y] = P[P_Y] + 0.5 * (v1 + vo1);
-    if (a.integrate_angle) P[P_ANG] = P[P_ANG] + 0.5 * (v2 + vo2);
-    if (!isfinite(P[P_X]) || !isfinite(P[P_Y]) || !isfinite(v0) || !isfinite(v1))
+    P[P_X] = nx_;
+    P[P_Y] = ny_;
+    if (a.integrate_angle) P[P_ANG] = P[P_ANG] + 0.5 * (v2 + u2);
+    if (!isfinite(nx_) || !isfinite(ny_) || !isfinite(v0) || !isfinite(v1))
       atomicOr(a.status, ST_NAN);
-    else if (P[P_X] < 0.0 || P[P_X] > (double)a.nx || P[P_Y] < 0.0 || P[P_Y] > (double)a.ny)
+    else if (nx_ < 0.0 || nx_ > (double)a.nx || ny_ < 0.0 || ny_ > (double)a.ny)
       atomicOr(a.status, ST_PARTICLE);
     if (rec && p < a.series_np) {
       double* r = a.series + rslot * a.series_len + 2 + 12LL * p;
-      r[0] = P[P_X]; r[1] = P[P_Y]; r[2] = P[P_ANG];
+      r[0] = nx_; r[1] = ny_; r[2] = P[P_ANG];
       r[3] = v0; r[4] = v1; r[5] = v2;
       r[6] = P[P_FX]; r[7] = P[P_FY]; r[8] = P[P_TZ];
       r[9] = fh0; r[10] = fh1; r[11] = fh2;
     }
+    const double tdx = nx_ - P[P_XT], tdy = ny_ - P[P_YT];
+    if (!(tdx * tdx + tdy * tdy <= 0.25 * SKIN * SKIN)) s_tiles = 1;
   }
   __syncthreads();
 
-  // ---- 4. tile candidate lists ----------------------------------------------
-  build_tiles(a, tid);
+  // ---- 3. tile candidate lists ---------------------------------------------
+  if (s_tiles) {
+    const int buf = 1 - *a.tile_cur;
+    int* cnt = a.tile_count + (long long)buf * a.ntiles;
+    for (int t = tid; t < a.ntiles; t += PBLK) cnt[t] = 0;
+    __syncthreads();
+    for (int p = tid; p < a.np; p += PBLK) {  // new centres, written above
+      double* P = a.ps + (long long)p * PS;
+      const double x = P[P_X], y = P[P_Y];
+      insert_tiles(a, p, x, y, P[P_D], buf);
+      P[P_XT] = x;
+      P[P_YT] = y;
+    }
+    __syncthreads();
+    if (tid == 0) *a.tile_cur = buf;
+  }
 }
 
-__global__ void __launch_bounds__(PBLK) k_tiles_only(const ParticleArgs a) {
-  build_tiles(a, threadIdx.x);
+// After set_particles / set_state: tile lists into buffer 0 (cleared by the
+// host) and a pair-list rebuild request for the next particle kernel.
+__global__ void __launch_bounds__(256) k_tiles_only(const ParticleArgs a) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.np; p += gridDim.x * blockDim.x) {
+    double* P = a.ps + (long long)p * PS;
+    insert_tiles(a, p, P[P_X], P[P_Y], P[P_D], 0);
+    P[P_XT] = P[P_X];
+    P[P_YT] = P[P_Y];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.tile_cur = 0;
+    *a.pair_rebuild = 1;
+  }
 }
 
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
-  k_particles<<<1, PBLK, 0, s>>>(a);
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !attr[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(k_particles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(PShared));
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) attr[dev] = true;
+  }
+  k_particles<<<1, PBLK, sizeof(PShared), s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tiles_only(const ParticleArgs& a, cudaStream_t s) {
-  k_tiles_only<<<1, PBLK, 0, s>>>(a);
+  const int blocks = (a.np + 255) / 256 > 0 ? (a.np + 255) / 256 : 1;
+  k_tiles_only<<<blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -241,6 +241,9 @@ def load_library():
         "lbm_get_state": ([vp, dp, dp, dp], ctypes.c_int),
         "lbm_set_state": ([vp, ctypes.c_int64, dp, dp, ctypes.c_int32, dp], ctypes.c_int),
         "lbm_get_status": ([vp], ctypes.c_int),
+        "lbm_get_stream": ([vp, P(vp)], ctypes.c_int),
+        "lbm_profile": ([vp, ctypes.c_int32], ctypes.c_int),
+        "lbm_profile_read": ([vp, dp, P(ctypes.c_int64)], ctypes.c_int),
         "lbm_strerror": ([ctypes.c_int], ctypes.c_char_p),
     }
     for name, (args, res) in sigs.items():
@@ -365,3 +368,19 @@ class Simulation:
 
     def status(self) -> int:
         return int(self.lib.lbm_get_status(self._h))
+
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for external events)."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.lbm_get_stream(self._h, ctypes.byref(s)), "lbm_get_stream")
+        return int(s.value or 0)
+
+    def profile(self, enable: bool) -> None:
+        self._check(self.lib.lbm_profile(self._h, 1 if enable else 0), "lbm_profile")
+
+    def profile_read(self):
+        """(particle_ms, lattice_ms), (particle_launches, lattice_launches)."""
+        ms = (ctypes.c_double * 2)()
+        n = (ctypes.c_int64 * 2)()
+        self._check(self.lib.lbm_profile_read(self._h, ms, n), "lbm_profile_read")
+        return (ms[0], ms[1]), (n[0], n[1])

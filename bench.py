@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Throughput of the hot path in MLUPS on one B200 (or N independent replicas).
+
+Workload (default): multi-particle sedimentation, 1024x2048 cells
+(1025x2049 = 2,100,225 nodes), 512 disks of diameter 16 at seeded
+non-overlapping positions in the upper half, density ratios U[1.01, 1.5],
+repulsion range 2, tau = 0.7, FP32 shifted populations; the plain FP64 path
+is timed on the same workload beside it.  One bench step = one time step of
+the whole lattice and all particles.  The per-step working set (two 76 MB
+population sweeps in FP32, 151 MB in FP64) exceeds the 126 MB L2, so no
+extra flush is needed between steps.
+
+Arms:
+  (default)          the CUDA library through its C ABI
+  --impl reference   the reference's algorithm on the host cores: the CPU
+                     oracle, a C restatement of the Fortran time step with
+                     its loop structure (the Fortran itself cannot be built
+                     in this image), single-threaded as the reference is
+
+Multi-GPU: the hot path does not shard (one simulation, one GPU); --gpus N
+runs N independent replicas (weak scaling), timed as the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_NODE = {0: 144.0, 1: 72.0}  # FP64 plain / FP32 shifted, Newtonian
+FALLBACK_HBM_GBS = 6650.0
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_lattice_fp32_cfg2.md")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="target CPU time of the bounded oracle sample")
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--ny", type=int, default=2048)
+    ap.add_argument("--particles", type=int, default=512)
+    return ap.parse_args()
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """dram read+write bytes per launch of the FP32 lattice kernel from the
+    committed ncu summary (a line 'traffic_bytes_per_launch: N'), or None."""
+    try:
+        with open(PROFILE_TRAFFIC) as fh:
+            for line in fh:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "20"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
+        thr = 0.5 * max(pw) if pw else 0.0
+        load = [num(r[1]) for r in rows if num(r[3]) is not None and num(r[3]) >= thr]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {
+            "sm_mhz": statistics.median(load or sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons,
+            "samples": len(rows),
+            "power_w_max": max(pw) if pw else None,
+        }
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(pkg, precision, args):
+    p, pin = pkg.cases.workload_cfg2(precision, args.nx, args.ny, args.particles)
+    p.series_capacity = 1024
+    return p, pin
+
+
+def time_steps(pkg, torch, sim, k):
+    ext = torch.cuda.ExternalStream(sim.stream())
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(ext)
+    sim.step(k)
+    t1.record(ext)
+    t1.synchronize()
+    return t0.elapsed_time(t1)
+
+
+def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False):
+    p, pin = workload(pkg, precision, args)
+    p.device = device
+    sim = pkg.Simulation(p)
+    sim.set_particles(pin)
+    sim.step(args.warmup)
+    sim.series()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(device) if clocks else None
+    if sampler:
+        sampler.start()
+    ms = time_steps(pkg, torch, sim, args.steps)
+    clk = sampler.stop() if sampler else None
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    status = sim.status()
+    # second pass: per-kernel events for the roofline
+    sim.profile(True)
+    sim.step(args.steps)
+    (pms, lms), (pn, ln) = sim.profile_read()
+    sim.profile(False)
+    sim.series()
+    parts = sim.particles()
+    sim.close()
+    nodes = (p.nx + 1) * (p.ny + 1)
+    return {
+        "ms": ms, "nodes": nodes, "lattice_ms": lms / max(ln, 1), "particle_ms": pms / max(pn, 1),
+        "launches": 2 * args.steps, "clocks": clk, "status": status,
+        "finite": bool(np.all(np.isfinite(parts[:, :6]))),
+    }
+
+
+def run_e2e(pkg, torch, args, device):
+    """Same metric through the public API with host buffers: the particle set
+    from pinned host memory, then every step lbm_step + a D2H read of the
+    particle state (the history the reference writes every step, C1:264)."""
+    p, pin = workload(pkg, 1, args)
+    p.device = device
+    sim = pkg.Simulation(p)
+    pin_h = torch.from_numpy(pin).pin_memory().numpy()
+    sim.set_particles(pin_h)
+    sim.step(args.warmup)
+    sim.particles()
+    ext = torch.cuda.ExternalStream(sim.stream())
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    k = args.steps
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    t0.record(ext)
+    sim.set_particles(pin_h)
+    out = None
+    for _ in range(k):
+        sim.step(1)
+        out = sim.particles()
+    t1.record(ext)
+    t1.synchronize()
+    wall = time.perf_counter() - w0
+    ms = t0.elapsed_time(t1)
+    sim.close()
+    nodes = (p.nx + 1) * (p.ny + 1)
+    return {
+        "value": nodes * k / (ms * 1e-3) / 1e6,
+        "unit": "MLUPS",
+        "h2d_bytes_per_step": int(pin.nbytes / k),
+        "d2h_bytes_per_step": int(out.nbytes),
+        "wall_s": wall,
+    }
+
+
+def cpu_baseline(pkg, args, seconds):
+    """The oracle (reference loop structure, one thread) on the same workload,
+    timed over a bounded number of whole time steps."""
+    from oracle.oracle import Oracle
+
+    p, pin = workload(pkg, 0, args)
+    nodes = (p.nx + 1) * (p.ny + 1)
+    need = 8 * nodes * (len(pin) + 40)
+    avail = 0
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    on_the_fly = 1 if avail and avail < 1.5 * need else 0
+    o = Oracle(p, phi_on_the_fly=on_the_fly)
+    o.set_particles(pin)
+    t = time.perf_counter()
+    o.step(1)
+    first = time.perf_counter() - t
+    n = max(1, min(50, int(seconds / max(first, 1e-3))))
+    t = time.perf_counter()
+    o.step(n)
+    dt = time.perf_counter() - t
+    o.close()
+    return {
+        "value": nodes * n / dt / 1e6,
+        "unit": "MLUPS",
+        "cores": 1,
+        "kind": "port",
+        "sample": (f"{n} full time steps of the {args.nx}x{args.ny}, {len(pin)}-disk workload "
+                   f"after 1 untimed step ({dt:.1f} s); PHI "
+                   + ("recomputed per loop (host memory)" if on_the_fly else
+                      "stored per particle over the lattice as in the reference")),
+    }
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_env()
+    pkg = importlib.import_module("2d_nnf_lbm_b200")
+    nodes = (args.nx + 1) * (args.ny + 1)
+    cfg = {
+        "workload": (f"multi-particle sedimentation {args.nx}x{args.ny} lattice "
+                     f"({nodes} nodes), {args.particles} disks D=16, tau=0.7, repulsion 2 lu"),
+        "nodes": nodes, "particles": args.particles, "precision": "fp32-shifted (fp64 beside)",
+        "l2": "working set per step 151 MB (fp32) / 302 MB (fp64) > 126 MB L2; no flush",
+        "parallelism": f"replicas x{world}",
+    }
+    metric = "MLUPS (FP32-shifted, multi-particle 1024x2048, 512 disks)"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = cpu_baseline(pkg, args, args.cpu_seconds)
+        line = {
+            "impl": "reference", "metric": metric, "value": base["value"], "unit": "MLUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = tdist
+    device = local if world > 1 else 0
+
+    r32 = run_gpu_path(pkg, torch, args, 1, device, world, dist, clocks=True)
+    r64 = run_gpu_path(pkg, torch, args, 0, device, world, dist)
+    e2e = run_e2e(pkg, torch, args, device)
+    if dist is not None:
+        t = torch.tensor([1.0 / e2e["value"]], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = world / float(t.item())
+
+    peak, peak_src = hbm_peak()
+    ach32 = BYTES_PER_NODE[1] * r32["nodes"] / (r32["lattice_ms"] * 1e-3) / 1e9
+    ach64 = BYTES_PER_NODE[0] * r64["nodes"] / (r64["lattice_ms"] * 1e-3) / 1e9
+    value = world * r32["nodes"] * args.steps / (r32["ms"] * 1e-3) / 1e6
+    value64 = world * r64["nodes"] * args.steps / (r64["ms"] * 1e-3) / 1e6
+    line = {
+        "metric": metric,
+        "value": value,
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r32["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic",
+        "config": cfg,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": ach32,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": ach32 / peak,
+            "traffic": profile_traffic(),
+            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+            else "fallback 6.65 TB/s",
+            "bytes_per_node": BYTES_PER_NODE[1],
+            "kernel": "k_lattice<float, STEP>",
+            "kernel_ms": r32["lattice_ms"],
+            "particle_kernel_ms": r32["particle_ms"],
+        },
+        "fp64": {
+            "value": value64, "unit": "MLUPS", "ms_per_step": r64["ms"] / args.steps,
+            "roofline_frac": ach64 / peak, "achieved_gbs": ach64,
+            "kernel_ms": r64["lattice_ms"], "bytes_per_node": BYTES_PER_NODE[0],
+        },
+        "fp32_over_fp64": value / value64,
+        "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
+        "gpu_launches": r32["launches"],
+        "clocks": r32["clocks"],
+        "status": {"fp32": r32["status"], "fp64": r64["status"],
+                   "finite": r32["finite"] and r64["finite"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pkg, args, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

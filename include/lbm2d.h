@@ -186,10 +186,15 @@ int lbm_series_record_len(lbm_sim* h, int32_t* len);
 /* Mean density SUM(RHO)/((NX+1)(NY+1)) of the current state (C1:318). */
 int lbm_get_mean_density(lbm_sim* h, double* avg);
 
-/* Checkpoint: the complete dynamic state.  f is 9*(NX+1)*(NY+1) doubles in
- * the reference's F(0:8,0:NX,0:NY) order holding the post-collision
- * populations of the next step; omega is (NX+1)*(NY+1) doubles (Bingham,
- * may be NULL otherwise); particles is np*LBM_STATE_PER doubles. */
+/* Checkpoint: the complete dynamic state of step KK, as the reference's
+ * restart dump holds it (C1:351-379): f is 9*(NX+1)*(NY+1) doubles in the
+ * F(0:8,0:NX,0:NY) order holding F after the boundary conditions of step KK;
+ * omega is OMEGA_BN, (NX+1)*(NY+1) doubles (Bingham; may be NULL otherwise);
+ * particles is np*LBM_STATE_PER doubles:
+ *   0 x 1 y 2 angle 3 u 4 v 5 omega 6-8 VP_OLD 9-11 FORCE 12-13 F_COL
+ *   14-16 F_H_IN 17 diam 18 rho_p 19 stale wall distance D_PW
+ * Unlike the reference dump, VP_OLD is kept, so a restart continues the
+ * internal-mass term exactly. */
 #define LBM_STATE_PER 20
 int lbm_get_state(lbm_sim* h, double* f, double* omega, double* particles);
 int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega,
@@ -197,6 +202,19 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega,
 
 /* Sticky device status (NaN, overflow, timeout); 0 when healthy. */
 int lbm_get_status(lbm_sim* h);
+
+/* The handle's CUDA stream (a cudaStream_t), so a caller can order its own
+ * work or record events against the library's kernels.  The reference has
+ * no counterpart (it is single-threaded host code). */
+int lbm_get_stream(lbm_sim* h, void** stream);
+
+/* Per-kernel device timing, for profiling the time loop (the reference only
+ * times the whole run, C1:148, C1:395-397).  While enabled, lbm_step records
+ * CUDA events around every launch; lbm_profile_read returns the summed
+ * device milliseconds and launch counts of the particle kernel [0] and the
+ * lattice kernel [1] since the last enable, and resets them. */
+int lbm_profile(lbm_sim* h, int32_t enable);
+int lbm_profile_read(lbm_sim* h, double* ms, int64_t* launches);
 
 const char* lbm_strerror(int code);
 

@@ -55,8 +55,9 @@ def compare_all(sim, ref, fields=("ux", "uy", "rho", "phi", "gx", "gy"), rtol=RT
         "force": ([6, 7], None),
         "torque": ([8], np.max(np.abs(rp[:, 6:8])) * float(d.max())),
         "collision": ([9, 10], np.max(np.abs(rp[:, 9:11])) + np.max(np.abs(rp[:, 6:8]))),
-        "internal": ([11, 12], None),
-        "internal_t": ([13], np.max(np.abs(rp[:, 11:13])) * float(d.max())),
+        # F_H_IN = (rho0/rho_p) M (v - v_old): velocity noise times the mass
+        "internal": ([11, 12], np.max(np.abs(rp[:, 14])) * np.max(np.abs(rp[:, 3:5]))),
+        "internal_t": ([13], np.max(np.abs(rp[:, 15])) * np.max(np.abs(rp[:, 3:5])) / float(d.max())),
         "mass": ([14, 15], None),
     }
     for name, (cols, sc) in groups.items():
@@ -105,8 +106,9 @@ def test_c6_bingham_fp64(pkg, cases, bc):
     p.bc = bc
     p.record_stress = 1
     sim, ref = pair(pkg, p, disk, 120)
-    compare_all(sim, ref)
-    close64(sim.field("omega"), ref.field("omega"), RTOL64, "omega")
+    # Papanastasiou with m = 5.5e6 amplifies ulp-level differences of sin()
+    compare_all(sim, ref, rtol=1e-8)
+    close64(sim.field("omega"), ref.field("omega"), 1e-8, "omega")
     for f in ("tau11", "tau22", "tau12"):
         close64(sim.field(f), ref.field(f), 1e-8, f)
     gi, ri = sim.image(), ref.image()
