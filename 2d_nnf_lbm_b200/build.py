@@ -46,34 +46,38 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    os.makedirs(BUILD_DIR, exist_ok=True)
+def build(verbose: bool = False, force: bool = False, out: str = OUT,
+          build_dir: str = BUILD_DIR, defines: tuple = ()) -> str:
+    """Compile and link; ``defines`` (e.g. ("LBM_MINB_F32=6",)) tune launch
+    bounds, ``out``/``build_dir`` place a variant elsewhere."""
+    os.makedirs(build_dir, exist_ok=True)
+    dflags = [f"-D{d}" for d in defines]
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "lbm2d.h"))
     objs = []
     logs = []
     for src, extra in SOURCES.items():
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        o = os.path.join(build_dir, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s, *headers, __file__]):
-            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", s, "-o", o]
+            cmd = [nvcc(), *ARCH, *COMMON, *dflags, *extra, "-c", s, "-o", o]
             r = subprocess.run(cmd, capture_output=True, text=True)
             logs.append(r.stdout + r.stderr)
             if r.returncode != 0:
                 sys.stderr.write(r.stdout + r.stderr)
                 raise RuntimeError(f"nvcc failed on {src}")
-    if force or _stale(OUT, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
+    if force or _stale(out, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", out, *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
-    with open(os.path.join(BUILD_DIR, "ptxas.log"), "a") as fh:
+    with open(os.path.join(build_dir, "ptxas.log"), "a") as fh:
         fh.write("".join(logs))
     if verbose:
         print("".join(logs))
-    return OUT
+    return out
 
 
 if __name__ == "__main__":

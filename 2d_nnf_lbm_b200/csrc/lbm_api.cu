@@ -25,6 +25,7 @@
 using namespace lbm;
 
 struct lbm_sim {
+  CUtensorMap tm[2];  // TMA descriptors of f[0], f[1] for the step kernel
   lbm_params p;
   cudaStream_t stream = nullptr;
   Geometry g{};
@@ -40,8 +41,10 @@ struct lbm_sim {
   // particles
   int np = 0;
   int np_cap = 0;
-  double* ps = nullptr;
-  unsigned long long* facc = nullptr;  // [np][6] FORCE accumulators
+  double* ps = nullptr;                // [PS][npad]
+  int npad = 32;
+  unsigned long long* facc = nullptr;  // [6][npad] FORCE accumulators
+  int* rec_slot = nullptr;
   int* tile_count = nullptr;
   int* tile_list = nullptr;
   int* tile_cur = nullptr;
@@ -151,16 +154,16 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.om_dst = h->om[h->cur ^ 1];
   a.ps = h->ps;
   a.np = h->np;
+  a.npad = h->npad;
+  a.rec_slot = h->rec_slot;
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
   a.tile_cur = h->tile_cur;
   a.tile_cap = h->tile_cap;
-  a.ntiles = h->g.nbx * h->g.nby;
+  a.ntiles = h->g.ltx * h->g.lty;
   a.facc = h->facc;
   a.kk = h->d_kk;
   a.mass_acc = h->series ? h->mass_acc : nullptr;
-  a.series_every = h->p.series_every;
-  a.series_cap = h->series_cap;
   a.status = h->d_status;
   a.rec = h->rec;
   return a;
@@ -170,14 +173,16 @@ ParticleArgs particle_args(lbm_sim* h) {
   ParticleArgs a{};
   a.ps = h->ps;
   a.np = h->np;
+  a.npad = h->npad;
+  a.rec_slot = h->rec_slot;
   a.facc = h->facc;
   a.decode_force = h->partials_valid ? 1 : 0;
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
   a.tile_cur = h->tile_cur;
   a.tile_cap = h->tile_cap;
-  a.ntiles = h->g.nbx * h->g.nby;
-  a.nbx = h->g.nbx;
+  a.ntiles = h->g.ltx * h->g.lty;
+  a.nbx = h->g.ltx;
   a.nbr = h->nbr;
   a.nbr_count = h->nbr_count;
   a.nbr_xy = h->nbr_xy;
@@ -216,14 +221,14 @@ ParticleArgs particle_args(lbm_sim* h) {
 cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
   if (h->prec == LBM_FP64) {
     switch (mode) {
-      case 0: return launch_step_fp64(a, h->stream);
+      case 0: return launch_step_fp64(a, &h->tm[h->cur], h->stream);
       case 1: return launch_output_fp64(a, h->stream);
       case 2: return launch_init_fp64(a, h->stream);
       default: return launch_restart_fp64(a, h->stream);
     }
   }
   switch (mode) {
-    case 0: return launch_step_fp32(a, h->stream);
+    case 0: return launch_step_fp32(a, &h->tm[h->cur], h->stream);
     case 1: return launch_output_fp32(a, h->stream);
     case 2: return launch_init_fp32(a, h->stream);
     default: return launch_restart_fp32(a, h->stream);
@@ -295,8 +300,10 @@ int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
   h->ncx = std::max(1, (int)std::floor((double)h->p.nx / h->cell_size) + 1);
   h->ncy = std::max(1, (int)std::floor((double)h->p.ny / h->cell_size) + 1);
   int rc;
-  const size_t npa = (size_t)std::max(np, 1);
+  h->npad = (std::max(np, 1) + 31) / 32 * 32;
+  const size_t npa = (size_t)h->npad;
   if ((rc = dalloc(&h->ps, npa * PS))) return rc;
+  CK(cudaMemsetAsync(h->ps, 0, sizeof(double) * npa * PS, h->stream));
   if ((rc = dalloc(&h->facc, npa * 6))) return rc;
   if ((rc = dalloc(&h->nbr, npa * MAX_NEIGH))) return rc;
   if ((rc = dalloc(&h->nbr_count, npa))) return rc;
@@ -304,7 +311,7 @@ int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
   CK(cudaMemsetAsync(h->facc, 0, sizeof(unsigned long long) * npa * 6, h->stream));
   CK(cudaMemsetAsync(h->nbr_count, 0, sizeof(int) * npa, h->stream));
   CK(cudaMemsetAsync(h->nbr_xy, 0, sizeof(double) * npa * 2, h->stream));
-  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.nbx * h->g.nby, h->stream));
+  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.ltx * h->g.lty, h->stream));
   h->series_np = std::max(0, std::min(h->p.series_particles, np));
   h->series_len = LBM_SERIES_HEAD + LBM_SERIES_PER * h->series_np;
   h->series_cap = std::max(1, h->p.series_capacity);
@@ -334,7 +341,7 @@ void particle_record(const lbm_params& p, double* P, double x, double y, double 
 
 int launch_tiles(lbm_sim* h) {
   ParticleArgs pa = particle_args(h);
-  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.nbx * h->g.nby, h->stream));
+  CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.ltx * h->g.lty, h->stream));
   CK(launch_tiles_only(pa, h->stream));
   return LBM_OK;
 }
@@ -343,19 +350,33 @@ int launch_tiles(lbm_sim* h) {
 // accumulators hold it (the next particle kernel decodes them on the
 // device), decode them here the same way.
 int read_particles(lbm_sim* h, std::vector<double>& buf) {
+  const size_t npad = (size_t)h->npad;
+  std::vector<double> soa(npad * PS);
+  CK(d2h(h, soa.data(), h->ps, soa.size() * sizeof(double)));
   buf.assign((size_t)std::max(h->np, 1) * PS, 0.0);
-  CK(d2h(h, buf.data(), h->ps, buf.size() * sizeof(double)));
+  for (int i = 0; i < h->np; ++i)
+    for (int f = 0; f < PS; ++f) buf[(size_t)i * PS + f] = soa[(size_t)f * npad + i];
   if (h->partials_valid && h->np > 0) {
-    std::vector<unsigned long long> acc((size_t)h->np * 6);
+    std::vector<unsigned long long> acc(npad * 6);
     CK(d2h(h, acc.data(), h->facc, acc.size() * sizeof(unsigned long long)));
     for (int i = 0; i < h->np; ++i) {
-      const unsigned long long* q = &acc[(size_t)i * 6];
       double* P = &buf[(size_t)i * PS];
-      P[P_FX] = decode_force(q[0], q[1]);
-      P[P_FY] = decode_force(q[2], q[3]);
-      P[P_TZ] = decode_force(q[4], q[5]);
+      P[P_FX] = decode_force(acc[i], acc[npad + i]);
+      P[P_FY] = decode_force(acc[2 * npad + i], acc[3 * npad + i]);
+      P[P_TZ] = decode_force(acc[4 * npad + i], acc[5 * npad + i]);
     }
   }
+  return LBM_OK;
+}
+
+// Upload np AoS records (PS doubles each) into the SoA device layout.
+int write_particles(lbm_sim* h, const std::vector<double>& buf) {
+  const size_t npad = (size_t)h->npad;
+  std::vector<double> soa(npad * PS, 0.0);
+  for (int i = 0; i < h->np; ++i)
+    for (int f = 0; f < PS; ++f) soa[(size_t)f * npad + i] = buf[(size_t)i * PS + f];
+  CK(h2d(h, h->ps, soa.data(), soa.size() * sizeof(double)));
+  CK(cudaStreamSynchronize(h->stream));
   return LBM_OK;
 }
 
@@ -411,6 +432,39 @@ cudaError_t record_event(lbm_sim* h) {
   return cudaEventRecord(h->ev[h->ev_used++], h->stream);
 }
 
+// Tensor maps over the population buffers, 3-D (x = pitch, y = NY+1,
+// z = 9 planes), box = one step-kernel tile of one plane.  The encoder comes
+// from the driver through the runtime, so no link against libcuda is needed.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int make_tensor_maps(lbm_sim* h) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      fn == nullptr || q != cudaDriverEntryPointSuccess)
+    return LBM_E_CUDA;
+  EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
+  const cuuint64_t dims[3] = {(cuuint64_t)h->g.pitch, (cuuint64_t)(h->p.ny + 1), 9};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->g.pitch * h->esz,
+                                 (cuuint64_t)h->g.plane * h->esz};
+  const cuuint32_t box[3] = {(cuuint32_t)step_box_width((int)h->esz),
+                             (cuuint32_t)step_box_rows((int)h->esz), 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  for (int b = 0; b < 2; ++b) {
+    CUresult r = enc(&h->tm[b],
+                     h->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                     3, h->f[b], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return LBM_E_CUDA;
+  }
+  return LBM_OK;
+}
+
 void destroy_buffers(lbm_sim* h) {
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->ev.clear();
@@ -421,6 +475,7 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->rec);
   dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
   dfree(h->tile_count); dfree(h->tile_list); dfree(h->tile_cur); dfree(h->pair_rebuild);
+  dfree(h->rec_slot);
   dfree(h->mass_acc);
   dfree(h->d_kk); dfree(h->stale_dpw);
   dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
@@ -519,6 +574,8 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   h->g.plane = (long long)h->g.pitch * (p.ny + 1);
   h->g.nbx = (p.nx + 1 + TX - 1) / TX;
   h->g.nby = (p.ny + 1 + TY - 1) / TY;
+  h->g.ltx = (p.nx + 1 + LTX - 1) / LTX;
+  h->g.lty = (p.ny + 1 + LTY - 1) / LTY;
   Model& m = h->m;
   m.bc = p.bc;
   m.bingham = p.rheology == LBM_BINGHAM;
@@ -580,11 +637,14 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if (m.record_stress &&
       cudaMalloc(&h->rec, (size_t)2 * 4 * h->g.plane * h->esz) != cudaSuccess)
     return fail(LBM_E_NOMEM);
-  const int ntiles = h->g.nbx * h->g.nby;
+  if ((rc = make_tensor_maps(h))) return fail(rc);
+  const int ntiles = h->g.ltx * h->g.lty;
   if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);
   if ((rc = dalloc(&h->tile_list, (size_t)2 * ntiles * h->tile_cap))) return fail(rc);
   if ((rc = dalloc(&h->tile_cur, 1))) return fail(rc);
   if ((rc = dalloc(&h->pair_rebuild, 1))) return fail(rc);
+  if ((rc = dalloc(&h->rec_slot, 1))) return fail(rc);
+  cudaMemsetAsync(h->rec_slot, 0xff, sizeof(int), h->stream);
   cudaMemsetAsync(h->tile_cur, 0, sizeof(int), h->stream);
   cudaMemsetAsync(h->pair_rebuild, 0, sizeof(int), h->stream);
   if ((rc = dalloc(&h->d_kk, 1))) return fail(rc);
@@ -638,7 +698,7 @@ int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
     const double* r = pin + (size_t)LBM_PIN * i;
     particle_record(h->p, &buf[(size_t)i * PS], r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7]);
   }
-  CK(h2d(h, h->ps, buf.data(), buf.size() * sizeof(double)));
+  if ((rc = write_particles(h, buf))) return rc;
   if ((rc = launch_tiles(h))) return rc;
   CK(cudaStreamSynchronize(h->stream));
   h->out_kk = -1;
@@ -873,7 +933,7 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, 
     P[P_FHX] = r[14]; P[P_FHY] = r[15]; P[P_FHT] = r[16];
     stale = r[19];
   }
-  CK(h2d(h, h->ps, buf.data(), buf.size() * sizeof(double)));
+  if ((rc = write_particles(h, buf))) return rc;
   CK(h2d(h, h->stale_dpw, &stale, sizeof(double)));
   const long long kkl = kk;
   CK(h2d(h, h->d_kk, &kkl, sizeof(long long)));

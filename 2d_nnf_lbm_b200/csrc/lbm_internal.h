@@ -6,21 +6,26 @@
 //                pitch = NX+1 rounded up to 32 elements so every row starts
 //                on a 128 B (FP32) / 256 B (FP64) boundary
 //   omega        om[2][NY+1][pitch]     per-node Bingham relaxation rate
-//   particles    ps[np][PS]             one 192 B FP64 record per disk
-//   force sums   facc[np][6]            exact fixed-point FORCE accumulators
+//   particles    ps[PS][npad]           structure of arrays, npad = np rounded to 32
+//   force sums   facc[6][npad]          exact fixed-point FORCE accumulators
 //   tile lists   tile_count[2][ntiles], tile_list[2][ntiles][tile_cap]
-//   pair lists   nbr_count[np], nbr[np][MAX_NEIGH]  (Verlet lists with skin)
+//   pair lists   nbr_count[npad], nbr[MAX_NEIGH][npad]  (Verlet lists with skin)
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace lbm {
 
-// Lattice tile = one thread block, one node per thread.
+// Scalar lattice kernels: one node per thread, blocks of TX x TY nodes.
 constexpr int TX = 32;
 constexpr int TY = 8;
 constexpr int TPB = TX * TY;
+// Particle candidate lists are kept per list tile of LTX x LTY nodes; a step
+// kernel tile (128 x 4 FP32 or 64 x 8 FP64 nodes) lies inside one list tile.
+constexpr int LTX = 128;
+constexpr int LTY = 8;
 constexpr int MAX_TILE_CAND = 32;   // particles that may touch one tile
 constexpr int MAX_PARTICLES = 4096; // particles per simulation (shared-memory staging)
 constexpr int MAX_NEIGH = 32;       // pair-list entries per particle
@@ -45,6 +50,13 @@ enum : int {
   PS
 };
 
+// Field f of particle p in the structure-of-arrays particle state.
+struct PRef {
+  double* base;  // &ps[p]
+  int stride;    // npad
+  __host__ __device__ double& operator[](int f) const { return base[(long long)f * stride]; }
+};
+
 // Sticky status bits.
 enum : int {
   ST_NAN = 1,
@@ -57,7 +69,8 @@ struct Geometry {
   int nx, ny;        // cells; nodes 0..nx, 0..ny
   int pitch;         // elements per row
   long long plane;   // elements per population plane = pitch*(ny+1)
-  int nbx, nby;      // tiles
+  int nbx, nby;      // scalar-kernel blocks
+  int ltx, lty;      // list tiles
 };
 
 struct Model {
@@ -76,18 +89,18 @@ struct Model {
 };
 
 struct ParticleArgs {
-  double* ps;
-  int np;
-  unsigned long long* facc;  // [np][6]
+  double* ps;                // [PS][npad]
+  int np, npad;
+  unsigned long long* facc;  // [6][npad]
   int decode_force;          // 1: FORCE = decoded accumulators (then zeroed)
   int* tile_count;           // [2][ntiles]
   int* tile_list;            // [2][ntiles][tile_cap]
   int* tile_cur;             // buffer the lattice kernel reads
   int tile_cap;
   int ntiles, nbx;
-  int* nbr;                  // [np][MAX_NEIGH]
-  int* nbr_count;            // [np]
-  double* nbr_xy;            // [np][2] centres at the last pair-list build
+  int* nbr;                  // [MAX_NEIGH][npad]
+  int* nbr_count;            // [npad]
+  double* nbr_xy;            // [2][npad] centres at the last pair-list build
   int* pair_rebuild;         // 1: rebuild the pair lists before use
   // repulsion
   int wall_model, contact;
@@ -99,6 +112,7 @@ struct ParticleArgs {
   double* stale_dpw;
   // bookkeeping
   long long* kk;
+  int* rec_slot;             // history slot of this step, -1 if none
   double* series;
   unsigned long long* mass_acc;  // [series_cap] fixed-point sum of rho - rho0
   int series_every, series_cap, series_len, series_np;
@@ -114,17 +128,17 @@ struct LatticeArgs {
   void* dst;             // f written
   const void* om_src;
   void* om_dst;
-  const double* ps;
-  int np;
+  const double* ps;      // [PS][npad]
+  int np, npad;
   const int* tile_count; // [2][ntiles]
   const int* tile_list;
   const int* tile_cur;
   int tile_cap;
   int ntiles;
-  unsigned long long* facc;
+  unsigned long long* facc;  // [6][npad]
   const long long* kk;
+  const int* rec_slot;   // history slot of this step (-1: none)
   unsigned long long* mass_acc;
-  int series_every, series_cap;
   int* status;
   // stress ring: 2 slots x (tau11, tau22, tau12, yield) fields
   void* rec;             // T[2][4][NY+1][pitch]
@@ -137,13 +151,18 @@ struct LatticeArgs {
 
 // Launchers (defined in lbm_fp64.cu / lbm_fp32.cu).
 cudaError_t launch_init_fp64(const LatticeArgs& a, cudaStream_t s);
-cudaError_t launch_step_fp64(const LatticeArgs& a, cudaStream_t s);
+cudaError_t launch_step_fp64(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s);
 cudaError_t launch_output_fp64(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_restart_fp64(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_init_fp32(const LatticeArgs& a, cudaStream_t s);
-cudaError_t launch_step_fp32(const LatticeArgs& a, cudaStream_t s);
+cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s);
 cudaError_t launch_output_fp32(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s);
+
+// TMA box of the step kernel: one tile row (128 FP32 / 64 FP64 nodes) plus
+// a 16-byte vector of halo on each side; 512 / row-width rows; one plane.
+inline int step_box_width(int esz) { return (esz == 8 ? 64 : 128) + 2 * (16 / esz); }
+inline int step_box_rows(int esz) { return 512 / (esz == 8 ? 64 : 128); }
 
 // Particle kernel (lbm_particles.cu).
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);

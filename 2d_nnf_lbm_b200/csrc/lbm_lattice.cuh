@@ -23,7 +23,10 @@
 //             force/torque/mass reductions in FP64.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "lbm_internal.h"
 
@@ -81,7 +84,7 @@ __device__ __forceinline__ float phi_float(float di, float dj, float R, float ze
   if (D <= -0.5f * zeta)
     phi = 0.0f;
   else if (fabsf(D) < 0.5f * zeta)
-    phi = 0.5f * (sinf(pi * D / zeta) + 1.0f);
+    phi = 0.5f * (__sinf(pi * D / zeta) + 1.0f);  // |argument| < pi/2
   else if (D >= 0.5f * zeta)
     phi = 1.0f;
   return phi;
@@ -204,76 +207,90 @@ __device__ __forceinline__ void collide_double(const Model& m, double* f, double
   }
 }
 
-// ---------------------------------------------------------------------------
-// The same collision on shifted FP32 populations h = f - w*rho0.  Moments of
-// h are m - rho0*(1,-2,1,0,...); the shift cancels in m - m_eq, and the
-// inverse transform adds back rho0*w_k*(36*d_mrt - 1) (zero for exact 1/36).
+// Relaxation rates of the FP32 update (s_e, s_eps, s_q, s_nu).
 struct Rates32 {
   float s1, s2, sq, sw;
 };
 
-__device__ __forceinline__ void collide_float(const Model& m, float* h, float drho, float rho,
-                                              float ux, float uy, float gx, float gy,
-                                              const Rates32& r, float dmrt, const float* shc,
-                                              bool want_stress, NodeOut& no) {
-  const float h0 = h[0], h1 = h[1], h2 = h[2], h3 = h[3], h4 = h[4], h5 = h[5], h6 = h[6],
-              h7 = h[7], h8 = h[8];
-  const float a1 = (h1 + h2) + (h3 + h4);
-  const float a5 = (h5 + h6) + (h7 + h8);
-  const float m1 = -4.0f * h0 - a1 + 2.0f * a5;
-  const float m2 = 4.0f * h0 - 2.0f * a1 + a5;
-  const float qx = (h5 - h6) - (h7 - h8);
-  const float qy = (h5 + h6) - (h7 + h8);
-  const float jx = (h1 - h3) + qx;
-  const float m4 = -2.0f * (h1 - h3) + qx;
-  const float jy = (h2 - h4) + qy;
-  const float m6 = -2.0f * (h2 - h4) + qy;
-  const float m7 = (h1 + h3) - (h2 + h4);
-  const float m8 = (h5 + h7) - (h6 + h8);
-  const float u2 = ux * ux + uy * uy;
-  const float ru2 = 3.0f * rho * u2;
-  const float e1 = -2.0f * drho + ru2;
-  const float e2 = drho - ru2;
+// ---------------------------------------------------------------------------
+// FP32 node update in moment space, on shifted populations h = f - w*rho0.
+// Moments of h are m - rho0*(1,-2,1,0,...); the shift cancels in m - m_eq,
+// and the inverse transform adds back rho0*w_k*(36*d_mrt - 1) (zero for an
+// exact 1/36).  The nine moments are formed once with pair sums/differences
+// and serve both the macroscopic variables and the collision, which then
+// works on the moments only.
+struct Mom32 {
+  float drho, jx, jy, m1, m2, m4, m6, m7, m8;
+};
+
+__device__ __forceinline__ Mom32 moments32(const float* h) {
+  Mom32 q;
+  const float a = h[1] + h[3], b = h[2] + h[4], c = h[5] + h[7], d = h[6] + h[8];
+  const float e = h[1] - h[3], g = h[2] - h[4], hh = h[5] - h[7], kk = h[6] - h[8];
+  const float ab = a + b, cd = c + d;
+  const float hmk = hh - kk, hpk = hh + kk;
+  q.drho = h[0] + (ab + cd);
+  q.jx = e + hmk;
+  q.jy = g + hpk;
+  q.m1 = fmaf(2.0f, cd, -ab) - 4.0f * h[0];
+  q.m2 = fmaf(4.0f, h[0], cd) - 2.0f * ab;
+  q.m4 = fmaf(-2.0f, e, hmk);
+  q.m6 = fmaf(-2.0f, g, hpk);
+  q.m7 = a - b;
+  q.m8 = c - d;
+  return q;
+}
+
+// Relax the moments (rates r, Guo forcing) and transform back to shifted
+// populations; optionally the Chai strain rate / Papanastasiou viscosity.
+__device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rho, float ux,
+                                        float uy, float gx, float gy, const Rates32& r,
+                                        bool want_stress, NodeOut& no, float* h) {
+  const float FX = rho * gx, FY = rho * gy;
+  const float uxx = ux * ux, uyy = uy * uy;
+  const float ru2 = 3.0f * rho * (uxx + uyy);
+  const float e1 = fmaf(-2.0f, q.drho, ru2);
+  const float e2 = q.drho - ru2;
   const float e4 = -rho * ux;
   const float e6 = -rho * uy;
-  const float e7 = rho * (ux * ux - uy * uy);
+  const float e7 = rho * (uxx - uyy);
   const float e8 = rho * (ux * uy);
-  const float FX = rho * gx, FY = rho * gy;
-  const float fu = FX * ux + FY * uy;
-  const float p0 = h0 + a1 + a5;  // conserved: post-collision mass = sum of populations
-  const float p1 = m1 + r.s1 * (e1 - m1) + (1.0f - 0.5f * r.s1) * (6.0f * fu);
-  const float p2 = m2 + r.s2 * (e2 - m2) - (1.0f - 0.5f * r.s2) * (6.0f * fu);
-  const float p3 = jx + FX;
-  const float p4 = m4 + r.sq * (e4 - m4) - (1.0f - 0.5f * r.sq) * FX;
-  const float p5 = jy + FY;
-  const float p6 = m6 + r.sq * (e6 - m6) - (1.0f - 0.5f * r.sq) * FY;
-  const float cw = 1.0f - 0.5f * r.sw;
-  const float p7 = m7 + r.sw * (e7 - m7) + cw * (2.0f * (FX * ux - FY * uy));
-  const float p8 = m8 + r.sw * (e8 - m8) + cw * (FY * ux + FX * uy);
-  const float b = 4.0f * p0 - p1 - 2.0f * p2;
-  const float c = 4.0f * p0 + 2.0f * p1 + p2;
-  const float x3 = 6.0f * p3 - 6.0f * p4;
-  const float y5 = 6.0f * p5 - 6.0f * p6;
-  const float d3 = 6.0f * p3 + 3.0f * p4;
-  const float d5 = 6.0f * p5 + 3.0f * p6;
-  h[0] = dmrt * (4.0f * (p0 - p1 + p2)) + shc[0];
-  h[1] = dmrt * (b + x3 + 9.0f * p7) + shc[1];
-  h[2] = dmrt * (b + y5 - 9.0f * p7) + shc[2];
-  h[3] = dmrt * (b - x3 + 9.0f * p7) + shc[3];
-  h[4] = dmrt * (b - y5 - 9.0f * p7) + shc[4];
-  h[5] = dmrt * (c + d3 + d5 + 9.0f * p8) + shc[5];
-  h[6] = dmrt * (c - d3 + d5 - 9.0f * p8) + shc[6];
-  h[7] = dmrt * (c - d3 - d5 + 9.0f * p8) + shc[7];
-  h[8] = dmrt * (c + d3 - d5 - 9.0f * p8) + shc[8];
+  const float fu = fmaf(FX, ux, FY * uy);
+  const float cw = 1.0f - 0.5f * r.sw, cq = 1.0f - 0.5f * r.sq;
+  const float p0 = q.drho;
+  const float p1 = fmaf(r.s1, e1 - q.m1, q.m1) + (6.0f - 3.0f * r.s1) * fu;
+  const float p2 = fmaf(r.s2, e2 - q.m2, q.m2) - (6.0f - 3.0f * r.s2) * fu;
+  const float p3 = q.jx + FX;
+  const float p5 = q.jy + FY;
+  const float p4 = fmaf(r.sq, e4 - q.m4, q.m4) - cq * FX;
+  const float p6 = fmaf(r.sq, e6 - q.m6, q.m6) - cq * FY;
+  const float p7 = fmaf(r.sw, e7 - q.m7, q.m7) + cw * (2.0f * fmaf(FX, ux, -FY * uy));
+  const float p8 = fmaf(r.sw, e8 - q.m8, q.m8) + cw * fmaf(FY, ux, FX * uy);
+  const float d = m.d_mrt_f;
+  const float A = fmaf(4.0f, p0, -p1) - 2.0f * p2;
+  const float B = fmaf(4.0f, p0, 2.0f * p1) + p2;
+  const float X = 6.0f * (p3 - p4), Y = 6.0f * (p5 - p6);
+  const float X2 = fmaf(6.0f, p3, 3.0f * p4), Y2 = fmaf(6.0f, p5, 3.0f * p6);
+  const float P7 = 9.0f * p7, P8 = 9.0f * p8;
+  const float AP = A + P7, AM = A - P7, BP = B + P8, BM = B - P8;
+  const float XpY = X2 + Y2, XmY = X2 - Y2;
+  h[0] = fmaf(d, 4.0f * (p0 - p1 + p2), m.shift_f[0]);
+  h[1] = fmaf(d, AP + X, m.shift_f[1]);
+  h[3] = fmaf(d, AP - X, m.shift_f[3]);
+  h[2] = fmaf(d, AM + Y, m.shift_f[2]);
+  h[4] = fmaf(d, AM - Y, m.shift_f[4]);
+  h[5] = fmaf(d, BP + XpY, m.shift_f[5]);
+  h[7] = fmaf(d, BP - XpY, m.shift_f[7]);
+  h[6] = fmaf(d, BM - XmY, m.shift_f[6]);
+  h[8] = fmaf(d, BM + XmY, m.shift_f[8]);
   if (!want_stress) return;
-  // D_ab = -d_mrt*1.5*sum_k c_a c_b [M^-1 S (m - m_eq)]_k*36 + forcing terms;
-  // closed form of C6:903-916 for S0 = S3 = S5 = 0
-  const float n1 = m1 - e1, n7 = m7 - e7, n8 = m8 - e8;
+  // closed form of the Chai strain rate (C6:903-916) with S0 = S3 = S5 = 0
+  const float n1 = q.m1 - e1, n7 = q.m7 - e7, n8 = q.m8 - e8;
   const float t1 = 9.0f * r.s1 * n1, t7 = 27.0f * r.sw * n7;
   const float gu = gx * ux + gy * uy;
-  float D11 = -dmrt * (t1 + t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gx * ux));
-  float D22 = -dmrt * (t1 - t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gy * uy));
-  float D12 = -54.0f * dmrt * r.sw * n8 + 0.75f * (-r.sw * (gx * uy + gy * ux));
+  float D11 = -d * (t1 + t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gx * ux));
+  float D22 = -d * (t1 - t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gy * uy));
+  float D12 = -54.0f * d * r.sw * n8 + 0.75f * (-r.sw * (gx * uy + gy * ux));
   const float NU = m.nu_f;
   no.t11 = NU * 2.0f * D11;
   no.t22 = NU * 2.0f * D22;
@@ -387,16 +404,24 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Exact, order-independent accumulation of a double into two int64 words:
 // v = hi*2^-20 + lo*2^-62 (|v| < 2^43).  Integer sums commute, so the
 // result does not depend on which warp adds first.
-__device__ __forceinline__ void facc_add(unsigned long long* acc, double v) {
+__device__ __forceinline__ void facc_add(unsigned long long* hi, unsigned long long* lo, double v) {
   const double t = v * FHI;
   const double h = floor(t);
   const double l = rint((t - h) * FLO);
-  atomicAdd(acc, (unsigned long long)(long long)h);
-  atomicAdd(acc + 1, (unsigned long long)(long long)l);
+  atomicAdd(hi, (unsigned long long)(long long)h);
+  atomicAdd(lo, (unsigned long long)(long long)l);
 }
 
+#ifndef LBM_MINB_F32
+#define LBM_MINB_F32 1
+#endif
+#ifndef LBM_MINB_F64
+#define LBM_MINB_F64 1
+#endif
+
 template <class T, int MODE>
-__global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
+__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_F32)
+    k_lattice(const LatticeArgs a) {
   constexpr bool F64 = sizeof(T) == 8;
   __shared__ int s_idx[MAX_TILE_CAND];
   __shared__ double s_px[MAX_TILE_CAND], s_py[MAX_TILE_CAND], s_pr[MAX_TILE_CAND];
@@ -406,7 +431,7 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   const int lane = tid & 31, warp = tid >> 5;
   const int i = blockIdx.x * TX + (tid & (TX - 1));
   const int j = blockIdx.y * TY + tid / TX;
-  const int tile = blockIdx.y * a.g.nbx + blockIdx.x;
+  const int tile = blockIdx.y * a.g.ltx + (blockIdx.x * TX) / LTX;
   const Geometry& g = a.g;
   const Model& m = a.m;
   (void)warp;
@@ -415,17 +440,19 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   // Every warp reads the count itself, so tiles without particles never wait
   // at a barrier; with particles, warp 0 stages them in shared memory sorted
   // by index (the last particle with PHI>0 sets G, C1:500-507).
-  long long kk = 0;
+  int kk = 0;        // parity of the step number
+  int rslot = -1;    // history slot of this step
   int ncand = 0;
   if (MODE != MODE_INIT) {
-    long long v = 0;
-    int c = 0, buf = 0;
+    int c = 0, buf = 0, kl = 0, rs = -1;
     if (lane == 0) {
-      if (MODE == MODE_STEP || MODE == MODE_RESTART) v = *a.kk;
+      if (MODE == MODE_STEP || MODE == MODE_RESTART) kl = (int)(*a.kk & 1);
+      if (MODE == MODE_STEP) rs = *a.rec_slot;
       buf = *a.tile_cur;
       c = a.tile_count[(long long)buf * a.ntiles + tile];
     }
-    kk = __shfl_sync(0xffffffffu, v, 0);
+    kk = __shfl_sync(0xffffffffu, kl, 0);
+    rslot = __shfl_sync(0xffffffffu, rs, 0);
     c = __shfl_sync(0xffffffffu, c, 0);
     buf = __shfl_sync(0xffffffffu, buf, 0);
     if (c > a.tile_cap) {
@@ -441,7 +468,7 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
 #pragma unroll 8
         for (int o = 0; o < 32; ++o) rank += (__shfl_sync(0xffffffffu, pv, o) < pv);
         if (lane < ncand) {
-          const double* p = a.ps + (long long)pv * PS;
+          const PRef p{const_cast<double*>(a.ps) + pv, a.npad};
           s_idx[rank] = pv;
           s_px[rank] = p[P_X];
           s_py[rank] = p[P_Y];
@@ -487,7 +514,14 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
 
   // ---- macroscopic variables (C1:1421-1439) ----------------------------
   T rho, drho, ux, uy;
+  Mom32 mq;
   if (initial) {
+    if (!F64) {
+      float hq[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) hq[k] = (float)f[k];
+      mq = moments32(hq);
+    }
     rho = F64 ? (T)m.rho0 : (T)m.rho0_f;
     drho = (T)0;
     ux = (T)0;
@@ -499,11 +533,15 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
     ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
     uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
   } else {
-    drho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
-    rho = (T)m.rho0_f + drho;
-    const T rinv = (T)__frcp_rn((float)rho);
-    ux = rinv * ((f[1] + f[5] + f[8]) - (f[6] + f[3] + f[7]));
-    uy = rinv * ((f[5] + f[2] + f[6]) - (f[7] + f[4] + f[8]));
+    float hq[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) hq[k] = (float)f[k];
+    mq = moments32(hq);
+    drho = (T)mq.drho;
+    rho = (T)(m.rho0_f + mq.drho);
+    const float rinv = __fdividef(1.0f, (float)rho);
+    ux = (T)(mq.jx * rinv);
+    uy = (T)(mq.jy * rinv);
   }
   if (!act) {
     rho = (T)1;
@@ -549,10 +587,11 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
       fy = warp_sum(fy);
       tz = warp_sum(tz);
       if (lane == 0) {
-        unsigned long long* acc = a.facc + (long long)s_idx[c] * 6;
-        facc_add(acc, fx);
-        facc_add(acc + 2, fy);
-        facc_add(acc + 4, tz);
+        unsigned long long* acc = a.facc + s_idx[c];
+        const long long st = a.npad;
+        facc_add(acc, acc + st, fx);
+        facc_add(acc + 2 * st, acc + 3 * st, fy);
+        facc_add(acc + 4 * st, acc + 5 * st, tz);
       }
     }
   }
@@ -582,13 +621,11 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   }
 
   // ---- mean density at history steps (C1:318): fixed-point, order-free ---
-  if (MODE == MODE_STEP && a.series_every > 0 && a.mass_acc != nullptr &&
-      (kk % a.series_every) == 0) {
+  if (MODE == MODE_STEP && rslot >= 0) {
     double s0 = warp_sum((double)drho);
     if (lane == 0) {
-      const long long slot = (kk / a.series_every - 1) % a.series_cap;
       const long long q = __double2ll_rn(s0 * MASS_FIX);
-      atomicAdd(a.mass_acc + slot, (unsigned long long)q);
+      atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
     }
   }
 
@@ -628,10 +665,8 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
       r.sq = m.sq_uni_f;
     }
     float hf[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) hf[k] = (float)f[k];
-    collide_float(m, hf, (float)drho, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy,
-                  r, m.d_mrt_f, m.shift_f, want_stress, no);
+    relax32(m, mq, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy, r, want_stress, no,
+            hf);
 #pragma unroll
     for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
   }
@@ -649,11 +684,448 @@ __global__ void __launch_bounds__(TPB) k_lattice(const LatticeArgs a) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised, TMA-pipelined time step (the launch lbm_step
+// uses).
+//
+// Tile = TR rows x TW nodes, one node per consumer thread.  Each population
+// plane of a tile is one TMA box of TR rows x (TW + 2H) elements, taken from
+// row j - c_y and starting H elements left of the tile (H = one 16-byte
+// vector), so the streamed value of node (i, j) sits at column i - c_x + H
+// of the box row.  One producer warp runs up to NSTAGE tiles ahead: it waits
+// until the consumers released a stage, stages the particles that touch the
+// tile, and issues the nine TMA boxes; the stage's "full" barrier completes
+// when both have landed.  The consumer warps wait on "full", compute their
+// nodes, release the stage on its "empty" barrier and store.  No block-wide
+// barrier is taken inside the loop.  Boxes that reach past the lattice are
+// zero-filled by the TMA unit; the nodes on the lattice edge gather their
+// populations from global memory with the boundary conditions instead.
+constexpr int STEP_CONSUMERS = 512;              // consumer threads (16 warps)
+constexpr int STEP_TPB = STEP_CONSUMERS + 32;    // + one producer warp
+
+template <class T>
+struct Stage {
+  static constexpr int H = 16 / (int)sizeof(T);               // halo: one 16-byte vector
+  static constexpr int TW = sizeof(T) == 8 ? 64 : 128;        // nodes per tile row
+  static constexpr int TR = STEP_CONSUMERS / TW;              // tile rows (8 or 4)
+  static constexpr int BW = TW + 2 * H;                       // box width (544 bytes)
+  static constexpr int PLANE = TR * BW;                       // elements per plane box
+  static constexpr int BYTES = 9 * PLANE * (int)sizeof(T);
+};
+
+#ifndef LBM_STEP_STAGES
+#define LBM_STEP_STAGES 3
+#endif
+constexpr int NSTAGE = LBM_STEP_STAGES;
+
+// Particles touching one tile, staged by the producer warp (one per stage).
+struct TileCand {
+  double px[MAX_TILE_CAND], py[MAX_TILE_CAND], pr[MAX_TILE_CAND];
+  double pu[MAX_TILE_CAND], pv[MAX_TILE_CAND], pw[MAX_TILE_CAND];
+  int idx[MAX_TILE_CAND];
+  int n;
+};
+
+template <class T>
+constexpr int step_smem() {
+  return NSTAGE * Stage<T>::BYTES + 2 * 8 * NSTAGE + 64 + NSTAGE * (int)sizeof(TileCand);
+}
+
+// Bounded wait on an mbarrier phase; false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+        "selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// (x, y) += (sx, sy) on a row of width ntx, wrapping x.
+__device__ __forceinline__ void tile_advance(int& x, int& y, int sx, int sy, int ntx) {
+  x += sx;
+  y += sy;
+  if (x >= ntx) {
+    x -= ntx;
+    ++y;
+  }
+}
+
+// The nine plane boxes of tile (bx, by) into a stage (one thread).
+template <class T>
+__device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, uint32_t mbar,
+                                         int bx, int by) {
+  using ST = Stage<T>;
+  const int x = bx * ST::TW - ST::H;  // a multiple of H: 16-byte aligned
+  const int y0 = by * ST::TR;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int cy = (k == 2 || k == 5 || k == 6) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0);
+    const uint32_t d = dst + (uint32_t)(k * ST::PLANE * (int)sizeof(T));
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(d),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y0 - cy), "r"(k), "r"(mbar)
+        : "memory");
+  }
+}
+
+// The producer warp stages the candidate particles of the list tile that
+// contains tile (bx, by).
+template <class T>
+__device__ __forceinline__ void stage_candidates(const LatticeArgs& a, int bx, int by, int buf,
+                                                 TileCand& C, int lane) {
+  using ST = Stage<T>;
+  const int lt = ((by * ST::TR) / LTY) * a.g.ltx + (bx * ST::TW) / LTX;
+  const long long tbase = (long long)buf * a.ntiles + lt;
+  int c = a.tile_count[tbase];
+  if (c > a.tile_cap) {
+    if (lane == 0) atomicOr(a.status, ST_OVERFLOW);
+    c = a.tile_cap;
+  }
+  if (lane < c) {
+    const int pv = a.tile_list[tbase * a.tile_cap + lane];
+    const PRef p{const_cast<double*>(a.ps) + pv, a.npad};
+    C.idx[lane] = pv;
+    C.px[lane] = p[P_X];
+    C.py[lane] = p[P_Y];
+    C.pr[lane] = 0.5 * p[P_D];
+    C.pu[lane] = p[P_U];
+    C.pv[lane] = p[P_V];
+    C.pw[lane] = p[P_W];
+  }
+  if (lane == 0) C.n = c;
+}
+
+#ifndef LBM_STEP_MINB_F32
+#define LBM_STEP_MINB_F32 2
+#endif
+#ifndef LBM_STEP_MINB_F64
+#define LBM_STEP_MINB_F64 1
+#endif
+
+template <class T>
+__global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 : LBM_STEP_MINB_F32)
+    k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm) {
+  constexpr bool F64 = sizeof(T) == 8;
+  constexpr uint32_t WAIT = 1u << 20;
+  using ST = Stage<T>;
+  extern __shared__ __align__(128) unsigned char s_raw[];
+  const T* stage = reinterpret_cast<const T*>(s_raw);
+  const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(s_raw);
+  const uint32_t full0 = s_base + NSTAGE * ST::BYTES;  // NSTAGE "full" barriers
+  const uint32_t empty0 = full0 + 8 * NSTAGE;          // NSTAGE "empty" barriers
+  TileCand* cands = reinterpret_cast<TileCand*>(s_raw + NSTAGE * ST::BYTES + 16 * NSTAGE + 64);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const Geometry& g = a.g;
+  const Model& m = a.m;
+  const int ntx = (g.nx + 1 + ST::TW - 1) / ST::TW;
+  const int nty = (g.ny + 1 + ST::TR - 1) / ST::TR;
+  const int sx = (int)gridDim.x % ntx, sy = (int)gridDim.x / ntx;
+
+  if (tid == 0) {
+    for (int st = 0; st < NSTAGE; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * st) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0 + 8 * st),
+                   "r"(STEP_CONSUMERS / 32)
+                   : "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == STEP_CONSUMERS / 32) {
+    // ================= producer warp =====================================
+    int bu = 0;
+    if (lane == 0) bu = *a.tile_cur;
+    const int buf = __shfl_sync(0xffffffffu, bu, 0);
+    int bx = (int)blockIdx.x % ntx, by = (int)blockIdx.x / ntx;
+    int sidx = 0;
+    uint32_t epar = 0;  // per-stage parity of the next "empty" completion
+    uint32_t fpar = 0;  // per-stage parity of the next "full" completion
+    for (int n = 0; by < nty; ++n) {
+      bool ok = true;
+      if (n >= NSTAGE) {
+        if (lane == 0) {
+          ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+          if (!ok) atomicOr(a.status, ST_TIMEOUT);
+        }
+        epar ^= 1u << sidx;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          // consumers gave up: let the boxes already in flight land (bounded)
+          if (lane == 0) {
+            for (int st = 0; st < NSTAGE; ++st)
+              mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
+          }
+          return;
+        }
+      }
+      stage_candidates<T>(a, bx, by, buf, cands[sidx], lane);
+      __syncwarp();
+      if (lane == 0) {
+        // boxes reaching past the lattice are filled with zeros; they still
+        // deliver their full byte count
+        const uint32_t fb = full0 + 8 * sidx;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                     "r"((uint32_t)ST::BYTES)
+                     : "memory");
+        tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
+      }
+      fpar ^= 1u << sidx;
+      sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
+      tile_advance(bx, by, sx, sy, ntx);
+    }
+    return;
+  }
+
+  // ================= consumer warps ========================================
+  int kpar, rslot;
+  {
+    int kl = 0, rs = -1;
+    if (lane == 0) {
+      kl = (int)(*a.kk & 1);
+      rs = *a.rec_slot;
+    }
+    kpar = __shfl_sync(0xffffffffu, kl, 0);
+    rslot = __shfl_sync(0xffffffffu, rs, 0);
+  }
+  const int tr = tid / ST::TW, tc = tid - tr * ST::TW;  // row and column in the tile
+  const T* __restrict__ src = static_cast<const T*>(a.src);
+  T* __restrict__ dst = static_cast<T*>(a.dst);
+  const long long P = g.plane;
+  const int pt = g.pitch;
+  int bx = (int)blockIdx.x % ntx, by = (int)blockIdx.x / ntx;
+  int sidx = 0;
+  uint32_t fpar = 0;  // per-stage parity of the next "full" completion
+
+  for (; by < nty; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1), tile_advance(bx, by, sx, sy, ntx)) {
+    const int i = bx * ST::TW + tc;
+    const int j = by * ST::TR + tr;
+    const long long nd = (long long)j * pt + i;
+    // A warp lies in one tile row: warp-uniform "has a lattice node".
+    const bool warp_live = (j <= g.ny) && (bx * ST::TW + (tc & ~31) <= g.nx);
+    if (!mbar_wait(full0 + 8 * sidx, (fpar >> sidx) & 1u, WAIT)) {
+      if (lane == 0) atomicOr(a.status, ST_TIMEOUT);
+      return;
+    }
+    fpar ^= 1u << sidx;
+    if (!warp_live) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
+      continue;
+    }
+    const TileCand& C = cands[sidx];
+
+    // ---- streaming + boundary conditions --------------------------------
+    // Nodes inside the lattice take the streamed values from the stage;
+    // nodes on its edge gather theirs with the boundary conditions.
+    const bool act = (i <= g.nx) && (j <= g.ny);
+    const bool edge = (i == 0) || (i >= g.nx) || (j == 0) || (j >= g.ny);
+    T f[9];
+    if (!edge) {
+      const T* q = stage + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
+      f[0] = q[0];
+      f[1] = q[ST::PLANE - 1];
+      f[2] = q[2 * ST::PLANE];
+      f[3] = q[3 * ST::PLANE + 1];
+      f[4] = q[4 * ST::PLANE];
+      f[5] = q[5 * ST::PLANE - 1];
+      f[6] = q[6 * ST::PLANE + 1];
+      f[7] = q[7 * ST::PLANE + 1];
+      f[8] = q[8 * ST::PLANE - 1];
+    } else if (act) {
+      pull_bc<T>(src, g, m.bc, i, j, f);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = (T)0;
+    }
+
+    // ---- macroscopic variables (C1:1421-1439) ---------------------------
+    T rho, drho, ux, uy;
+    Mom32 mq;
+    if (F64) {
+      rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+      drho = rho - (T)m.rho0;
+      const T rinv = (T)1.0 / rho;
+      ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
+      uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
+    } else {
+      float hq[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) hq[k] = (float)f[k];
+      mq = moments32(hq);
+      drho = (T)mq.drho;
+      rho = (T)(m.rho0_f + mq.drho);
+      const float rinv = __fdividef(1.0f, (float)rho);
+      ux = (T)(mq.jx * rinv);
+      uy = (T)(mq.jy * rinv);
+    }
+    if (!act) {
+      rho = (T)1;
+      drho = (T)0;
+      ux = uy = (T)0;
+    }
+
+    // ---- SPM body force (the highest-index particle with PHI>0 sets G,
+    //      C1:500-507) and force sums ---------------------------------------
+    T gx = (T)0, gy = (T)0;
+    int gbest = -1;
+    const int ncand = C.n;
+    for (int c = 0; c < ncand; ++c) {
+      double fx = 0.0, fy = 0.0, tz = 0.0;
+      bool hit = false;
+      if (act) {
+        const double di = (double)i - C.px[c];
+        const double dj = (double)j - C.py[c];
+        T phi;
+        if (F64)
+          phi = (T)phi_double(di, dj, C.pr[c], m.zeta, m.pi);
+        else
+          phi = (T)phi_float((float)di, (float)dj, (float)C.pr[c], m.zeta_f, m.pi_f);
+        if (phi > (T)0) {
+          hit = true;
+          const T uxp = (T)C.pu[c] - (T)C.pw[c] * (T)dj;
+          const T uyp = (T)C.pv[c] + (T)C.pw[c] * (T)di;
+          if (C.idx[c] > gbest) {
+            gbest = C.idx[c];
+            gx = phi * (uxp - ux);
+            gy = phi * (uyp - uy);
+          }
+          const T rp = rho * phi;
+          fx = (double)(rp * (ux - uxp));
+          fy = (double)(rp * (uy - uyp));
+          tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
+        }
+      }
+      if (__any_sync(0xffffffffu, hit)) {
+        fx = warp_sum(fx);
+        fy = warp_sum(fy);
+        tz = warp_sum(tz);
+        if (lane == 0) {
+          unsigned long long* acc = a.facc + C.idx[c];
+          const long long st = a.npad;
+          facc_add(acc, acc + st, fx);
+          facc_add(acc + 2 * st, acc + 3 * st, fy);
+          facc_add(acc + 4 * st, acc + 5 * st, tz);
+        }
+      }
+    }
+    // the stage and its candidates are consumed
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
+
+    // ---- mean density at history steps (C1:318): fixed-point, order-free -
+    if (rslot >= 0) {
+      const double sd = warp_sum((double)drho);
+      if (lane == 0) {
+        const long long q = __double2ll_rn(sd * MASS_FIX);
+        atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
+      }
+    }
+    if (!act) continue;
+
+    // ---- velocity correction (C1:1138-1152) and collision of the next step
+    const T uxc = ux + (T)0.5 * (gx + (T)0.0);
+    const T uyc = uy + (T)0.5 * (gy + (T)0.0);
+    const bool want_stress = m.bingham || m.record_stress;
+    NodeOut no;
+    no.omega = m.omega;
+    no.yield = 0;
+    no.t11 = no.t22 = no.t12 = 0.0;
+    T omn = (T)m.omega;
+    if (m.bingham) omn = static_cast<const T*>(a.om_src)[nd];
+    if (F64) {
+      double S[9];
+      if (m.bingham) {
+        rates_double(m, (double)omn, S);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) S[k] = m.S_uni[k];
+      }
+      double fd[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) fd[k] = (double)f[k];
+      collide_double(m, fd, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, S,
+                     want_stress, no);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = (T)fd[k];
+    } else {
+      Rates32 r;
+      r.s1 = m.s_e_f;
+      r.s2 = m.s_eps_f;
+      if (m.bingham) {
+        const float w = (float)omn;
+        r.sw = w;
+        r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : m.sq_uni_f;
+      } else {
+        r.sw = m.omega_f;
+        r.sq = m.sq_uni_f;
+      }
+      float hf[9];
+      relax32(m, mq, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy, r, want_stress, no,
+              hf);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dst[k * P + nd] = f[k];
+    if (m.bingham) static_cast<T*>(a.om_dst)[nd] = (T)no.omega;
+    if (m.record_stress) {
+      const int slot = (kpar + 1) & 1;
+      T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * P;
+      rec[nd] = (T)no.t11;
+      rec[P + nd] = (T)no.t22;
+      rec[2 * P + nd] = (T)no.t12;
+      rec[3 * P + nd] = (T)no.yield;
+    }
+  }
+}
+
+template <class T>
+cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s) {
+  using ST = Stage<T>;
+  constexpr int SMEM = step_smem<T>();
+  static int grid_of[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (grid_of[dev] == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_step<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<T>, STEP_TPB, SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    grid_of[dev] = (per_sm > 0 ? per_sm : 1) * sms;
+  }
+  const int ntiles = ((a.g.nx + 1 + ST::TW - 1) / ST::TW) * ((a.g.ny + 1 + ST::TR - 1) / ST::TR);
+  const int grid = ntiles < grid_of[dev] ? ntiles : grid_of[dev];
+  k_step<T><<<grid, STEP_TPB, SMEM, s>>>(a, *tm);
+  return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t launch_mode(const LatticeArgs& a, cudaStream_t s, int mode) {
   dim3 grid(a.g.nbx, a.g.nby);
   switch (mode) {
-    case MODE_STEP: k_lattice<T, MODE_STEP><<<grid, TPB, 0, s>>>(a); break;
+    case MODE_STEP: return cudaErrorInvalidValue;  // launch_step below
     case MODE_OUTPUT: k_lattice<T, MODE_OUTPUT><<<grid, TPB, 0, s>>>(a); break;
     case MODE_INIT: k_lattice<T, MODE_INIT><<<grid, TPB, 0, s>>>(a); break;
     default: k_lattice<T, MODE_RESTART><<<grid, TPB, 0, s>>>(a); break;

@@ -69,7 +69,7 @@ __device__ __forceinline__ void insert_tiles(const ParticleArgs& a, int p, doubl
   int i0 = max((int)ceil(x - r), 0), i1 = min((int)floor(x + r), a.nx);
   int j0 = max((int)ceil(y - r), 0), j1 = min((int)floor(y + r), a.ny);
   if (!(i0 <= i1 && j0 <= j1) || !isfinite(x) || !isfinite(y)) return;
-  const int tx0 = i0 / TX, ty0 = j0 / TY, ntx = i1 / TX - tx0 + 1, nty = j1 / TY - ty0 + 1;
+  const int tx0 = i0 / LTX, ty0 = j0 / LTY, ntx = i1 / LTX - tx0 + 1, nty = j1 / LTY - ty0 + 1;
   int* cnt = a.tile_count + (long long)buf * a.ntiles;
   int* lst = a.tile_list + (long long)buf * a.ntiles * a.tile_cap;
   const int nt = ntx * nty;
@@ -158,7 +158,7 @@ __device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
   __syncthreads();
   for (int p = tid; p < a.np; p += PBLK) {
     const double px = S.x[p], py = S.y[p], pd = S.d[p];
-    int* nb = a.nbr + (long long)p * MAX_NEIGH;
+    int nbl[MAX_NEIGH];
     int nn = 0;
     const int key = S.key[p];
     const int cx = key % a.ncx, cy = key / a.ncx;
@@ -174,19 +174,20 @@ __device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
           if (dx * dx + dy * dy > lim * lim) continue;
           if (nn < MAX_NEIGH) {
             int k = nn++;
-            while (k > 0 && nb[k - 1] > q) {
-              nb[k] = nb[k - 1];
+            while (k > 0 && nbl[k - 1] > q) {
+              nbl[k] = nbl[k - 1];
               --k;
             }
-            nb[k] = q;
+            nbl[k] = q;
           } else {
             atomicOr(a.status, ST_OVERFLOW);
           }
         }
       }
+    for (int k = 0; k < nn; ++k) a.nbr[(long long)k * a.npad + p] = nbl[k];
     a.nbr_count[p] = nn;
-    a.nbr_xy[2 * p] = px;
-    a.nbr_xy[2 * p + 1] = py;
+    a.nbr_xy[p] = px;
+    a.nbr_xy[a.npad + p] = py;
   }
 }
 
@@ -198,32 +199,37 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
   const int tid = threadIdx.x;
 
   if (tid == 0) {
-    s_kk = *a.kk + 1;
-    *a.kk = s_kk;
+    const long long k1 = *a.kk + 1;
+    s_kk = k1;
+    *a.kk = k1;
     s_pairs = *a.pair_rebuild;
     s_tiles = 0;
+    const bool r = a.series != nullptr && a.series_every > 0 && (k1 % a.series_every) == 0;
+    const long long slot = r ? (k1 / a.series_every - 1) % a.series_cap : -1;
+    *a.rec_slot = (int)slot;  // read by the lattice kernel of this step
+    if (r) {
+      a.series[slot * a.series_len + 0] = (double)k1;
+      a.series[slot * a.series_len + 1] = __longlong_as_double(0x7ff8000000000000LL);
+      if (a.mass_acc) a.mass_acc[slot] = 0ull;
+    }
   }
   const double stale = *a.stale_dpw;  // D_PW left over from the previous call
   __syncthreads();
   const long long kk = s_kk;
   const bool rec = a.series != nullptr && a.series_every > 0 && (kk % a.series_every) == 0;
   const long long rslot = rec ? (kk / a.series_every - 1) % a.series_cap : 0;
-  if (rec && tid == 0) {
-    a.series[rslot * a.series_len + 0] = (double)kk;
-    a.series[rslot * a.series_len + 1] = __longlong_as_double(0x7ff8000000000000LL);
-    if (a.mass_acc) a.mass_acc[rslot] = 0ull;
-  }
 
   // ---- 0. FORCE of the last lattice step; stage centres ------------------
   for (int p = tid; p < a.np; p += PBLK) {
-    double* P = a.ps + (long long)p * PS;
+    const PRef P{a.ps + p, a.npad};
     if (a.decode_force) {
-      unsigned long long* acc = a.facc + (long long)p * 6;
-      const double fx = decode_force(acc[0], acc[1]);
-      const double fy = decode_force(acc[2], acc[3]);
-      const double tz = decode_force(acc[4], acc[5]);
+      unsigned long long* acc = a.facc + p;
+      const long long st = a.npad;
+      const double fx = decode_force(acc[0], acc[st]);
+      const double fy = decode_force(acc[2 * st], acc[3 * st]);
+      const double tz = decode_force(acc[4 * st], acc[5 * st]);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) acc[k] = 0ull;
+      for (int k = 0; k < 6; ++k) acc[k * st] = 0ull;
       P[P_FX] = fx;
       P[P_FY] = fy;
       P[P_TZ] = tz;
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     S.y[p] = y;
     S.d[p] = P[P_D];
     if (a.np > 1) {
-      const double ddx = x - a.nbr_xy[2 * p], ddy = y - a.nbr_xy[2 * p + 1];
+      const double ddx = x - a.nbr_xy[p], ddy = y - a.nbr_xy[a.npad + p];
       if (!(ddx * ddx + ddy * ddy <= 0.25 * SKIN * SKIN)) s_pairs = 1;
     }
   }
@@ -248,14 +254,22 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
 
   // ---- 2. repulsion, Newton-Euler update, history -------------------------
   for (int p = tid; p < a.np; p += PBLK) {
-    double* P = a.ps + (long long)p * PS;
+    const PRef P{a.ps + p, a.npad};
+    // issue every global load of this disk before the dependent arithmetic
+    const double u0 = P[P_U], u1 = P[P_V], u2 = P[P_W];
+    const double uo0 = P[P_UO], uo1 = P[P_VO], uo2 = P[P_WO];
+    const double frx = P[P_FX], fry = P[P_FY], frt = P[P_TZ];
+    const double rhop = P[P_RHO], M = P[P_M], I = P[P_I], ang = P[P_ANG];
+    const double xt = P[P_XT], yt = P[P_YT];
     const double px = S.x[p], py = S.y[p], pd = S.d[p];
     double fcx = 0.0, fcy = 0.0;
     if (a.np > 1) {
-      const int* nb = a.nbr + (long long)p * MAX_NEIGH;
       const int nn = a.nbr_count[p];
+      int nbl[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) nbl[k] = k < nn ? a.nbr[(long long)k * a.npad + p] : 0;
       for (int k = 0; k < nn; ++k) {
-        const int q = nb[k];
+        const int q = k < 8 ? nbl[k] : a.nbr[(long long)k * a.npad + p];
         double F[2];
         if (q < p) {
           pair_force(a, S.x[q], S.y[q], S.d[q], px, py, pd, stale, F);
@@ -310,15 +324,13 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
 
     // Newton-Euler with internal-mass correction (C1:250-258, C6:312)
     const double RHO0 = a.rho0;
-    const double rr = RHO0 / P[P_RHO];
-    const double M = P[P_M], I = P[P_I];
-    const double u0 = P[P_U], u1 = P[P_V], u2 = P[P_W];
-    const double fh0 = rr * M * (u0 - P[P_UO]);
-    const double fh1 = rr * M * (u1 - P[P_VO]);
-    const double fh2 = rr * I * (u2 - P[P_WO]);
-    const double v0 = u0 + P[P_FX] / M + fh0 / M + fcx / M;
-    const double v1 = u1 + P[P_FY] / M + fh1 / M + (1.0 - RHO0 / P[P_RHO]) * a.gravity + fcy / M;
-    const double v2 = u2 + P[P_TZ] / I + fh2 / I;
+    const double rr = RHO0 / rhop;
+    const double fh0 = rr * M * (u0 - uo0);
+    const double fh1 = rr * M * (u1 - uo1);
+    const double fh2 = rr * I * (u2 - uo2);
+    const double v0 = u0 + frx / M + fh0 / M + fcx / M;
+    const double v1 = u1 + fry / M + fh1 / M + (1.0 - RHO0 / rhop) * a.gravity + fcy / M;
+    const double v2 = u2 + frt / I + fh2 / I;
     const double nx_ = px + 0.5 * (v0 + u0);
     const double ny_ = py + 0.5 * (v1 + u1);
     P[P_FHX] = fh0;
@@ -332,19 +344,20 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     P[P_W] = v2;
     P[P_X] = nx_;
     P[P_Y] = ny_;
-    if (a.integrate_angle) P[P_ANG] = P[P_ANG] + 0.5 * (v2 + u2);
+    const double nang = a.integrate_angle ? ang + 0.5 * (v2 + u2) : ang;
+    if (a.integrate_angle) P[P_ANG] = nang;
     if (!isfinite(nx_) || !isfinite(ny_) || !isfinite(v0) || !isfinite(v1))
       atomicOr(a.status, ST_NAN);
     else if (nx_ < 0.0 || nx_ > (double)a.nx || ny_ < 0.0 || ny_ > (double)a.ny)
       atomicOr(a.status, ST_PARTICLE);
     if (rec && p < a.series_np) {
       double* r = a.series + rslot * a.series_len + 2 + 12LL * p;
-      r[0] = nx_; r[1] = ny_; r[2] = P[P_ANG];
+      r[0] = nx_; r[1] = ny_; r[2] = nang;
       r[3] = v0; r[4] = v1; r[5] = v2;
-      r[6] = P[P_FX]; r[7] = P[P_FY]; r[8] = P[P_TZ];
+      r[6] = frx; r[7] = fry; r[8] = frt;
       r[9] = fh0; r[10] = fh1; r[11] = fh2;
     }
-    const double tdx = nx_ - P[P_XT], tdy = ny_ - P[P_YT];
+    const double tdx = nx_ - xt, tdy = ny_ - yt;
     if (!(tdx * tdx + tdy * tdy <= 0.25 * SKIN * SKIN)) s_tiles = 1;
   }
   __syncthreads();
@@ -356,7 +369,7 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     for (int t = tid; t < a.ntiles; t += PBLK) cnt[t] = 0;
     __syncthreads();
     for (int p = tid; p < a.np; p += PBLK) {  // new centres, written above
-      double* P = a.ps + (long long)p * PS;
+      const PRef P{a.ps + p, a.npad};
       const double x = P[P_X], y = P[P_Y];
       insert_tiles(a, p, x, y, P[P_D], buf);
       P[P_XT] = x;
@@ -371,7 +384,7 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
 // host) and a pair-list rebuild request for the next particle kernel.
 __global__ void __launch_bounds__(256) k_tiles_only(const ParticleArgs a) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.np; p += gridDim.x * blockDim.x) {
-    double* P = a.ps + (long long)p * PS;
+    const PRef P{a.ps + p, a.npad};
     insert_tiles(a, p, P[P_X], P[P_Y], P[P_D], 0);
     P[P_XT] = P[P_X];
     P[P_YT] = P[P_Y];
