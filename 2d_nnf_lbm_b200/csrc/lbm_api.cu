@@ -1019,6 +1019,7 @@ const char* lbm_strerror(int code) {
     case LBM_E_STATE: return "call out of order";
     case LBM_E_PARTICLE: return "particle outside the lattice";
     case LBM_E_ABI: return "lbm_params.struct_size mismatch";
+    case LBM_E_SCRATCH: return "lattice or particle count exceeds the fixed no-alloc scratch";
     default: return "unknown error";
   }
 }

@@ -245,6 +245,7 @@ def load_library():
         "lbm_profile": ([vp, ctypes.c_int32], ctypes.c_int),
         "lbm_profile_read": ([vp, dp, P(ctypes.c_int64)], ctypes.c_int),
         "lbm_strerror": ([ctypes.c_int], ctypes.c_char_p),
+        "lbm_fields_noalloc": ([P(LbmParams), vp, ctypes.c_int32, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

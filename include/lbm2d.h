@@ -42,7 +42,8 @@ enum {
     LBM_E_OVERFLOW = -7,  /* a lattice tile is touched by too many particles  */
     LBM_E_STATE = -8,     /* call out of order (e.g. step before particles)   */
     LBM_E_PARTICLE = -9,  /* particle outside the lattice                     */
-    LBM_E_ABI = -10       /* struct_size does not match this library          */
+    LBM_E_ABI = -10,      /* struct_size does not match this library          */
+    LBM_E_SCRATCH = -11   /* input larger than lbm_fields_noalloc's scratch   */
 };
 
 /* ---- variant switches (compile-time PARAMETERs / IF(0|1) blocks upstream) */
@@ -217,6 +218,40 @@ int lbm_profile(lbm_sim* h, int32_t enable);
 int lbm_profile_read(lbm_sim* h, double* ms, int64_t* launches);
 
 const char* lbm_strerror(int code);
+
+/* Output fields of a state held in caller-owned device memory, computed
+ * without allocating anything (no counterpart in the reference).
+ *
+ * For drivers that must not allocate device memory while they run: one that
+ * has given all device memory to its own pool or to other solvers, or one
+ * that post-processes inside its time loop, where cudaMalloc/cudaFree would
+ * synchronise the whole device.  No simulation handle is needed.
+ *
+ *   p          nx, ny, zeta, pi are read (struct_size must match)
+ *   f          device, 9*(NX+1)*(NY+1) doubles: F after the boundary
+ *              conditions, F(0:8,0:NX,0:NY) order (as lbm_get_state gives it)
+ *   particles  device, np*LBM_PIN doubles (x, y, angle, u, v, omega, diam,
+ *              rho_p); may be NULL when np == 0
+ *   out        device, 7*(NX+1)*(NY+1) doubles: UX, UY, RHO, PHI, GX, GY as
+ *              lbm_get_field gives them, then the image code (10 particle
+ *              node, else 0), i fastest
+ *   stream     cudaStream_t to run on (NULL: the legacy default stream)
+ *
+ * The candidate lists of the solid-fraction evaluation live in a fixed
+ * static device array, so the lattice may hold at most LBM_NOALLOC_MAX_TILES
+ * tiles of 128 x 8 nodes (ceil((NX+1)/128) * ceil((NY+1)/8), e.g. 2047 x
+ * 8191) and at most LBM_NOALLOC_MAX_PARTICLES disks; larger inputs return
+ * LBM_E_SCRATCH before any work is queued.  Each call clears the scratch it
+ * uses, so nothing needs to start at zero.  The first call on a device also
+ * looks up the scratch address (make it before any stream capture starts on
+ * that device).  The scratch is shared by all calls on a device: calls that
+ * overlap in time on one device race and must be serialised by the caller.
+ * The call returns after its work on `stream` has finished; LBM_E_OVERFLOW
+ * if more than 32 disks touch one tile. */
+#define LBM_NOALLOC_MAX_TILES 16384
+#define LBM_NOALLOC_MAX_PARTICLES 4096
+int lbm_fields_noalloc(const lbm_params* p, const double* f, int32_t np,
+                       const double* particles, double* out, void* stream);
 
 #ifdef __cplusplus
 }
