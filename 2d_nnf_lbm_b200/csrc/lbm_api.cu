@@ -3,8 +3,8 @@
 //
 // Per time step the host enqueues two kernels on the handle's stream:
 //   k_particles  repulsion, Newton-Euler update, history, tile lists
-//   k_lattice    stream + BC + macro + SPM + force sums + correction +
-//                collision of the next step
+//   k_step       stream + BC + macro + SPM + force sums + correction +
+//                collision of the next step (persistent, TMA-fed)
 // The post-collision populations live in a ping-pong pair: after step K,
 // f[cur] holds f*(K+1) and f[cur^1] holds f*(K), from which the output
 // kernel re-derives the fields of step K (F after BC, rho, u, G, PHI) on
@@ -718,7 +718,7 @@ int lbm_step(lbm_sim* h, int32_t nsteps) {
       if (rc) return rc;
     }
     if (h->prof) {
-      if (h->ev_used + 3 > 3 * 4096) {
+      if (h->ev_used + 3 > 3 * 65536) {
         int rc = profile_flush(h);
         if (rc) return rc;
       }

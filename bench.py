@@ -40,13 +40,13 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_NODE = {0: 144.0, 1: 72.0}  # FP64 plain / FP32 shifted, Newtonian
 FALLBACK_HBM_GBS = 6650.0
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_lattice_fp32_cfg2.md")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_step_fp32_sedimentation_1024x2048.md")
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -190,7 +190,9 @@ def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     status = sim.status()
-    # second pass: per-kernel events for the roofline
+    # Per-kernel durations: an identical pass of the same number of steps
+    # with CUDA events recorded between the launches on the library's stream
+    # (events inside the timed pass itself would slow it by ~15%).
     sim.profile(True)
     sim.step(args.steps)
     (pms, lms), (pn, ln) = sim.profile_read()
@@ -238,7 +240,7 @@ def run_e2e(pkg, torch, args, device):
     return {
         "value": nodes * k / (ms * 1e-3) / 1e6,
         "unit": "MLUPS",
-        "h2d_bytes_per_step": int(pin.nbytes / k),
+        "h2d_bytes_per_step": pin.nbytes / k,
         "d2h_bytes_per_step": int(out.nbytes),
         "wall_s": wall,
     }
@@ -362,7 +364,7 @@ def main():
             "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
             else "fallback 6.65 TB/s",
             "bytes_per_node": BYTES_PER_NODE[1],
-            "kernel": "k_lattice<float, STEP>",
+            "kernel": "k_step<float>",
             "kernel_ms": r32["lattice_ms"],
             "particle_kernel_ms": r32["particle_ms"],
         },
