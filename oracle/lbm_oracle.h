@@ -9,9 +9,14 @@
  *
  * Parity pin: the reference Fortran cannot be compiled in this image (no
  * gfortran/flang).  The restatement is pinned against golden vectors that
- * tests/golden/make_golden.py produces by executing the unmodified
- * reference sources (parameter-patched in memory) with a Fortran-subset
- * interpreter; see tests/test_oracle_golden.py.
+ * tests/golden/make_golden.py produces by executing the reference's own
+ * C1, C6 and C3 sources (PARAMETERs shrunk in memory; the STOP at C3:202
+ * skipped) with the Fortran-subset translator tests/golden/f90run.py.  The
+ * oracle reproduces all four fixtures bit for bit
+ * (tests/test_oracle_golden.py).  Shared by translator and oracle, and so
+ * not independently checked: the reading of gfortran's arithmetic (REAL(4)
+ * literals, promotion, no contraction) and the zero start of the stale
+ * D_PW local.
  */
 #ifndef LBM_ORACLE_H
 #define LBM_ORACLE_H
