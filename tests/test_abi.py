@@ -95,3 +95,22 @@ def test_record_layout_constants(pkg):
         assert re.search(rf"#define {name} {val}\b", src), name
         assert getattr(pkg.lbm2d, name) == val
     assert np.dtype(np.float64).itemsize == 8
+
+
+def test_fortran_module_mirrors_header(pkg):
+    """include/lbm2d_mod.f90 binds every entry point and lays out LBM_PARAMS
+    field by field as lbm_params (no Fortran compiler here, so by text)."""
+    mod = open(os.path.join(ROOT, "include", "lbm2d_mod.f90")).read().upper()
+    bound = set(n.lower() for n in re.findall(r"NAME='(LBM_[A-Z_0-9]+)'", mod))
+    assert set(declared_functions()) == bound
+    body = re.search(r"TYPE, BIND\(C\) :: LBM_PARAMS(.*?)END TYPE", mod, re.S).group(1)
+    names = []
+    for line in body.replace("&\n", " ").split("\n"):
+        if "::" in line:
+            for n in line.split("::", 1)[1].split(","):
+                n = n.strip()
+                m = re.match(r"([A-Z_0-9]+)(\((\d+)\))?", n)
+                if m:
+                    names += [m.group(1).lower()] * (1 if not m.group(3) else 1)
+    fields = [f for f, _ in pkg.LbmParams._fields_]
+    assert names == fields
