@@ -155,14 +155,16 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.ps = h->ps;
   a.np = h->np;
   a.npad = h->npad;
-  a.rec_slot = h->rec_slot;
+  a.step = h->kk;
+  a.rec_slot = -1;
+  if (h->series && h->p.series_every > 0 && h->kk > 0 && h->kk % h->p.series_every == 0)
+    a.rec_slot = (int)((h->kk / h->p.series_every - 1) % h->series_cap);
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
   a.tile_cur = h->tile_cur;
   a.tile_cap = h->tile_cap;
   a.ntiles = h->g.ltx * h->g.lty;
   a.facc = h->facc;
-  a.kk = h->d_kk;
   a.mass_acc = h->series ? h->mass_acc : nullptr;
   a.status = h->d_status;
   a.rec = h->rec;
@@ -261,6 +263,8 @@ int drain_series(lbm_sim* h) {
     CK(d2h(h, dst, h->series + slot * len, (size_t)cnt * len * sizeof(double)));
     acc.resize(cnt);
     CK(d2h(h, acc.data(), h->mass_acc + slot, (size_t)cnt * sizeof(unsigned long long)));
+    // the slots start at zero again before the ring comes back to them
+    CK(cudaMemsetAsync(h->mass_acc + slot, 0, (size_t)cnt * sizeof(unsigned long long), h->stream));
     // AvgDen = rho0 + sum(rho - rho0)/N from the fixed-point accumulator
     for (long long q = 0; q < cnt; ++q)
       dst[q * len + 1] = h->p.rho0 + (double)(long long)acc[q] / MASS_FIX / nn;
@@ -641,11 +645,11 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   const int ntiles = h->g.ltx * h->g.lty;
   if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);
   if ((rc = dalloc(&h->tile_list, (size_t)2 * ntiles * h->tile_cap))) return fail(rc);
-  if ((rc = dalloc(&h->tile_cur, 1))) return fail(rc);
+  if ((rc = dalloc(&h->tile_cur, 2))) return fail(rc);
   if ((rc = dalloc(&h->pair_rebuild, 1))) return fail(rc);
   if ((rc = dalloc(&h->rec_slot, 1))) return fail(rc);
   cudaMemsetAsync(h->rec_slot, 0xff, sizeof(int), h->stream);
-  cudaMemsetAsync(h->tile_cur, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(h->tile_cur, 0, 2 * sizeof(int), h->stream);
   cudaMemsetAsync(h->pair_rebuild, 0, sizeof(int), h->stream);
   if ((rc = dalloc(&h->d_kk, 1))) return fail(rc);
   if ((rc = dalloc(&h->stale_dpw, 1))) return fail(rc);

@@ -95,7 +95,7 @@ struct ParticleArgs {
   int decode_force;          // 1: FORCE = decoded accumulators (then zeroed)
   int* tile_count;           // [2][ntiles]
   int* tile_list;            // [2][ntiles][tile_cap]
-  int* tile_cur;             // buffer the lattice kernel reads
+  int* tile_cur;             // [2]: list buffer valid for step k at [k&1]
   int tile_cap;
   int ntiles, nbx;
   int* nbr;                  // [MAX_NEIGH][npad]
@@ -132,12 +132,12 @@ struct LatticeArgs {
   int np, npad;
   const int* tile_count; // [2][ntiles]
   const int* tile_list;
-  const int* tile_cur;
+  const int* tile_cur;   // [2]: list buffer valid for step k at [k&1]
   int tile_cap;
   int ntiles;
   unsigned long long* facc;  // [6][npad]
-  const long long* kk;
-  const int* rec_slot;   // history slot of this step (-1: none)
+  long long step;        // lattice step of this launch
+  int rec_slot;          // history slot of this step (-1: none)
   unsigned long long* mass_acc;
   int* status;
   // stress ring: 2 slots x (tau11, tau22, tau12, yield) fields

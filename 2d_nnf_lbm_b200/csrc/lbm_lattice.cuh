@@ -446,9 +446,9 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
   if (MODE != MODE_INIT) {
     int c = 0, buf = 0, kl = 0, rs = -1;
     if (lane == 0) {
-      if (MODE == MODE_STEP || MODE == MODE_RESTART) kl = (int)(*a.kk & 1);
-      if (MODE == MODE_STEP) rs = *a.rec_slot;
-      buf = *a.tile_cur;
+      if (MODE == MODE_STEP || MODE == MODE_RESTART) kl = (int)(a.step & 1);
+      if (MODE == MODE_STEP) rs = a.rec_slot;
+      buf = a.tile_cur[a.step & 1];
       c = a.tile_count[(long long)buf * a.ntiles + tile];
     }
     kk = __shfl_sync(0xffffffffu, kl, 0);
@@ -702,6 +702,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
 // zero-filled by the TMA unit; the nodes on the lattice edge gather their
 // populations from global memory with the boundary conditions instead.
 constexpr int STEP_CONSUMERS = 512;              // consumer threads (16 warps)
+constexpr int STEP_MASKS = 64;  // 32-tile masks per CTA: up to 2048 tiles split by pass
 constexpr int STEP_TPB = STEP_CONSUMERS + 32;    // + one producer warp
 
 template <class T>
@@ -725,6 +726,7 @@ struct TileCand {
   double pu[MAX_TILE_CAND], pv[MAX_TILE_CAND], pw[MAX_TILE_CAND];
   int idx[MAX_TILE_CAND];
   int n;
+  int bx, by;  // the tile in this stage
 };
 
 template <class T>
@@ -751,17 +753,6 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
 
-// (x, y) += (sx, sy) on a row of width ntx, wrapping x.
-__device__ __forceinline__ void tile_advance(int& x, int& y, int sx, int sy, int ntx) {
-  x += sx;
-  y += sy;
-  if (x >= ntx) {
-    x -= ntx;
-    ++y;
-  }
-}
-
-// The nine plane boxes of tile (bx, by) into a stage (one thread).
 template <class T>
 __device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, uint32_t mbar,
                                          int bx, int by) {
@@ -786,6 +777,14 @@ template <class T>
 __device__ __forceinline__ void stage_candidates(const LatticeArgs& a, int bx, int by, int buf,
                                                  TileCand& C, int lane) {
   using ST = Stage<T>;
+  if (lane == 0) {
+    C.bx = bx;
+    C.by = by;
+  }
+  if (buf < 0) {  // a tile that no disk can reach
+    if (lane == 0) C.n = 0;
+    return;
+  }
   const int lt = ((by * ST::TR) / LTY) * a.g.ltx + (bx * ST::TW) / LTX;
   const long long tbase = (long long)buf * a.ntiles + lt;
   int c = a.tile_count[tbase];
@@ -833,7 +832,6 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
   const Model& m = a.m;
   const int ntx = (g.nx + 1 + ST::TW - 1) / ST::TW;
   const int nty = (g.ny + 1 + ST::TR - 1) / ST::TR;
-  const int sx = (int)gridDim.x % ntx, sy = (int)gridDim.x / ntx;
 
   if (tid == 0) {
     for (int st = 0; st < NSTAGE; ++st) {
@@ -846,82 +844,120 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
   }
   __syncthreads();
 
+  __shared__ unsigned s_mask[STEP_MASKS];
   if (warp == STEP_CONSUMERS / 32) {
     // ================= producer warp =====================================
-    int bu = 0;
-    if (lane == 0) bu = *a.tile_cur;
-    const int buf = __shfl_sync(0xffffffffu, bu, 0);
-    int bx = (int)blockIdx.x % ntx, by = (int)blockIdx.x / ntx;
+    // Pass 0: tiles that no disk can reach by the lists of the previous step
+    // (a disk moves less than the Verlet skin between list builds); they need
+    // nothing from this step's particle kernel, which may still be running.
+    // Pass 1: after griddepcontrol.wait, the tiles that list disks, with the
+    // disks' state of this step and the lists valid for it.
+    int bo = 0;
+    if (lane == 0) bo = a.tile_cur[(a.step - 1) & 1];
+    const int buf_old = __shfl_sync(0xffffffffu, bo, 0);
+    // which of this CTA's tiles list disks: one bit per tile, 32 tiles per
+    // load across the lanes (n-th tile of the CTA: t = blockIdx.x + n*gridDim.x)
+    const int nmine = (ntx * nty - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int nch = (nmine + 31) / 32;
+    const bool split = nch <= STEP_MASKS;  // else every tile waits for the particle kernel
+    if (split) {
+      for (int ch = 0; ch < nch; ++ch) {
+        const int nn = ch * 32 + lane;
+        bool listed = false;
+        if (nn < nmine) {
+          const int t = (int)blockIdx.x + nn * (int)gridDim.x;
+          const int by = t / ntx, bx = t - by * ntx;
+          const int lt = ((by * ST::TR) / LTY) * g.ltx + (bx * ST::TW) / LTX;
+          listed = a.tile_count[(long long)buf_old * a.ntiles + lt] > 0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, listed);
+        if (lane == 0) s_mask[ch] = m;
+      }
+      __syncwarp();
+    }
+    int buf = -1;
     int sidx = 0;
     uint32_t epar = 0;  // per-stage parity of the next "empty" completion
     uint32_t fpar = 0;  // per-stage parity of the next "full" completion
-    for (int n = 0; by < nty; ++n) {
-      bool ok = true;
-      if (n >= NSTAGE) {
-        if (lane == 0) {
-          ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
-          if (!ok) atomicOr(a.status, ST_TIMEOUT);
-        }
-        epar ^= 1u << sidx;
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) {
-          // consumers gave up: let the boxes already in flight land (bounded)
+    int n = 0;          // tiles issued
+    bool alive = true;
+    for (int pass = split ? 0 : 1; pass < 2 && alive; ++pass) {
+      if (pass == 1) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        int bn = 0;
+        if (lane == 0) bn = a.tile_cur[a.step & 1];
+        buf = __shfl_sync(0xffffffffu, bn, 0);
+      }
+      for (int ch = 0; ch < nch && alive; ++ch) {
+        const unsigned valid = ch * 32 + 32 <= nmine ? 0xffffffffu : ((1u << (nmine - ch * 32)) - 1u);
+        unsigned todo = !split ? valid : (pass == 0 ? ~s_mask[ch] & valid : s_mask[ch]);
+        while (todo) {
+        const int bit = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int t = (int)blockIdx.x + (ch * 32 + bit) * (int)gridDim.x;
+        const int by = t / ntx, bx = t - by * ntx;
+        if (n >= NSTAGE) {
+          bool ok = true;
           if (lane == 0) {
-            for (int st = 0; st < NSTAGE; ++st)
-              mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
+            ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+            if (!ok) atomicOr(a.status, ST_TIMEOUT);
           }
-          return;
+          epar ^= 1u << sidx;
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) {
+            // consumers gave up: let the boxes already in flight land (bounded)
+            if (lane == 0) {
+              for (int st = 0; st < NSTAGE; ++st)
+                mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
+            }
+            alive = false;
+            break;
+          }
+        }
+        stage_candidates<T>(a, bx, by, buf, cands[sidx], lane);
+        __syncwarp();
+        if (lane == 0) {
+          // boxes reaching past the lattice are filled with zeros; they still
+          // deliver their full byte count
+          const uint32_t fb = full0 + 8 * sidx;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                       "r"((uint32_t)ST::BYTES)
+                       : "memory");
+          tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
+        }
+        fpar ^= 1u << sidx;
+        sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
+        ++n;
         }
       }
-      stage_candidates<T>(a, bx, by, buf, cands[sidx], lane);
-      __syncwarp();
-      if (lane == 0) {
-        // boxes reaching past the lattice are filled with zeros; they still
-        // deliver their full byte count
-        const uint32_t fb = full0 + 8 * sidx;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
-                     "r"((uint32_t)ST::BYTES)
-                     : "memory");
-        tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
-      }
-      fpar ^= 1u << sidx;
-      sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
-      tile_advance(bx, by, sx, sy, ntx);
     }
     return;
   }
 
   // ================= consumer warps ========================================
-  int kpar, rslot;
-  {
-    int kl = 0, rs = -1;
-    if (lane == 0) {
-      kl = (int)(*a.kk & 1);
-      rs = *a.rec_slot;
-    }
-    kpar = __shfl_sync(0xffffffffu, kl, 0);
-    rslot = __shfl_sync(0xffffffffu, rs, 0);
-  }
+  const int kpar = (int)(a.step & 1), rslot = a.rec_slot;
+  bool waited = false;  // griddepcontrol.wait done (before the first force sum)
   const int tr = tid / ST::TW, tc = tid - tr * ST::TW;  // row and column in the tile
   const T* __restrict__ src = static_cast<const T*>(a.src);
   T* __restrict__ dst = static_cast<T*>(a.dst);
   const long long P = g.plane;
   const int pt = g.pitch;
-  int bx = (int)blockIdx.x % ntx, by = (int)blockIdx.x / ntx;
+  const int nmine = (ntx * nty - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
 
-  for (; by < nty; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1), tile_advance(bx, by, sx, sy, ntx)) {
-    const int i = bx * ST::TW + tc;
-    const int j = by * ST::TR + tr;
-    const long long nd = (long long)j * pt + i;
-    // A warp lies in one tile row: warp-uniform "has a lattice node".
-    const bool warp_live = (j <= g.ny) && (bx * ST::TW + (tc & ~31) <= g.nx);
+  for (int n = 0; n < nmine; ++n, sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
     if (!mbar_wait(full0 + 8 * sidx, (fpar >> sidx) & 1u, WAIT)) {
       if (lane == 0) atomicOr(a.status, ST_TIMEOUT);
       return;
     }
     fpar ^= 1u << sidx;
+    const int bx = cands[sidx].bx, by = cands[sidx].by;  // set by the producer
+    const int i = bx * ST::TW + tc;
+    const int j = by * ST::TR + tr;
+    const long long nd = (long long)j * pt + i;
+    // A warp lies in one tile row: warp-uniform "has a lattice node".
+    const bool warp_live = (j <= g.ny) && (bx * ST::TW + (tc & ~31) <= g.nx);
     if (!warp_live) {
       __syncwarp();
       if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
@@ -1014,6 +1050,10 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
         fx = warp_sum(fx);
         fy = warp_sum(fy);
         tz = warp_sum(tz);
+        if (!waited) {  // the particle kernel has zeroed the accumulators
+          asm volatile("griddepcontrol.wait;" ::: "memory");
+          waited = true;
+        }
         if (lane == 0) {
           unsigned long long* acc = a.facc + C.idx[c];
           const long long st = a.npad;
@@ -1113,12 +1153,27 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    grid_of[dev] = (per_sm > 0 ? per_sm : 1) * sms;
+    // one SM stays free for the particle kernel that runs beside the
+    // particle-free tiles (it fills an SM's register file on its own)
+    grid_of[dev] = (per_sm > 0 ? per_sm : 1) * (sms > 1 ? sms - 1 : 1);
   }
   const int ntiles = ((a.g.nx + 1 + ST::TW - 1) / ST::TW) * ((a.g.ny + 1 + ST::TR - 1) / ST::TR);
   const int grid = ntiles < grid_of[dev] ? ntiles : grid_of[dev];
-  k_step<T><<<grid, STEP_TPB, SMEM, s>>>(a, *tm);
-  return cudaGetLastError();
+  // Programmatic dependent launch: the kernel may start as soon as the
+  // particle kernel before it on the stream allows (griddepcontrol.
+  // launch_dependents); it waits for that kernel (griddepcontrol.wait) before
+  // the tiles that need its results.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(STEP_TPB);
+  cfg.dynamicSmemBytes = SMEM;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_step<T>, a, *tm);
 }
 
 template <class T>

@@ -197,6 +197,8 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
   __shared__ long long s_kk;
   __shared__ int s_pairs, s_tiles;
   const int tid = threadIdx.x;
+  // the lattice kernel of this step may start its particle-free tiles now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (tid == 0) {
     const long long k1 = *a.kk + 1;
@@ -210,7 +212,6 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     if (r) {
       a.series[slot * a.series_len + 0] = (double)k1;
       a.series[slot * a.series_len + 1] = __longlong_as_double(0x7ff8000000000000LL);
-      if (a.mass_acc) a.mass_acc[slot] = 0ull;
     }
   }
   const double stale = *a.stale_dpw;  // D_PW left over from the previous call
@@ -363,8 +364,13 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
   __syncthreads();
 
   // ---- 3. tile candidate lists ---------------------------------------------
+  // The lattice kernel of this step, already running, sorts its tiles by the
+  // lists of the previous step (tile_cur[(k-1)&1]); a rebuild goes into the
+  // other buffer, published as tile_cur[k&1].
+  const int cur = a.tile_cur[(s_kk - 1) & 1];
+  if (!s_tiles && tid == 0) a.tile_cur[s_kk & 1] = cur;
   if (s_tiles) {
-    const int buf = 1 - *a.tile_cur;
+    const int buf = 1 - cur;
     int* cnt = a.tile_count + (long long)buf * a.ntiles;
     for (int t = tid; t < a.ntiles; t += PBLK) cnt[t] = 0;
     __syncthreads();
@@ -376,7 +382,7 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
       P[P_YT] = y;
     }
     __syncthreads();
-    if (tid == 0) *a.tile_cur = buf;
+    if (tid == 0) a.tile_cur[s_kk & 1] = buf;
   }
 }
 
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(256) k_tiles_only(const ParticleArgs a) {
     P[P_YT] = P[P_Y];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *a.tile_cur = 0;
+    a.tile_cur[0] = a.tile_cur[1] = 0;
     *a.pair_rebuild = 1;
   }
 }
