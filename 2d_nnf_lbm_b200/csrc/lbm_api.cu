@@ -70,6 +70,9 @@ struct lbm_sim {
   int64_t drained_kk = 0;
   std::vector<double> host_series;
   size_t host_series_read = 0;
+  // COMPUTEERROR: velocity of the previous call, per-block partial sums
+  double* u0 = nullptr;       // [2][nodes]
+  double* err_part = nullptr;
   // output scratch
   double* out = nullptr;
   double* out_f = nullptr;
@@ -483,13 +486,74 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->mass_acc);
   dfree(h->d_kk); dfree(h->stale_dpw);
   dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
+  dfree(h->u0); dfree(h->err_part);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+constexpr int ERR_BLOCKS = 592, ERR_TPB = 256;
+
+// Per block: sum of |u - u0|^2 and |u|^2 over a fixed strided set of nodes
+// reduced by a fixed tree (deterministic), and u0 = u.
+__global__ void __launch_bounds__(ERR_TPB) k_error(const double* ux, const double* uy,
+                                                   double* u0, double* v0, long long nn,
+                                                   double* part) {
+  __shared__ double s1[ERR_TPB], s2[ERR_TPB];
+  double e1 = 0.0, e2 = 0.0;
+  for (long long n = blockIdx.x * (long long)ERR_TPB + threadIdx.x; n < nn;
+       n += (long long)gridDim.x * ERR_TPB) {
+    const double x = ux[n], y = uy[n], dx = x - u0[n], dy = y - v0[n];
+    e1 += dx * dx + dy * dy;
+    e2 += x * x + y * y;
+    u0[n] = x;
+    v0[n] = y;
+  }
+  s1[threadIdx.x] = e1;
+  s2[threadIdx.x] = e2;
+  __syncthreads();
+  for (int w = ERR_TPB / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s1[0];
+    part[2 * blockIdx.x + 1] = s2[0];
+  }
 }
 
 }  // namespace
 
 extern "C" {
+
+int lbm_compute_error(lbm_sim* h, double* er) {
+  if (!h || !er) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  const long long nn = nodes(h);
+  if (!h->u0) {
+    int rc = dalloc(&h->u0, (size_t)2 * nn);
+    if (!rc) rc = dalloc(&h->err_part, (size_t)2 * ERR_BLOCKS);
+    if (rc) return rc;
+    // the previous velocity starts as INITIALIZE's, zero (C1:154-155)
+    CK(cudaMemsetAsync(h->u0, 0, sizeof(double) * 2 * nn, h->stream));
+  }
+  int rc = compute_output(h, false);  // corrected velocity of step kk in out[0], out[1]
+  if (rc) return rc;
+  k_error<<<ERR_BLOCKS, ERR_TPB, 0, h->stream>>>(h->out, h->out + nn, h->u0, h->u0 + nn, nn,
+                                                 h->err_part);
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)2 * ERR_BLOCKS);
+  CK(d2h(h, part.data(), h->err_part, part.size() * sizeof(double)));
+  double e1 = 0.0, e2 = 0.0;
+  for (int b = 0; b < ERR_BLOCKS; ++b) {
+    e1 += part[2 * (size_t)b];
+    e2 += part[2 * (size_t)b + 1];
+  }
+  *er = std::sqrt(e1 / e2);
+  return refreshed_status(h);
+}
 
 int lbm_params_init(lbm_params* p) {
   if (!p) return LBM_E_INVALID;

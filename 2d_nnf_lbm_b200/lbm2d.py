@@ -238,6 +238,7 @@ def load_library():
         "lbm_get_series": ([vp, dp, ctypes.c_int32, ip], ctypes.c_int),
         "lbm_series_record_len": ([vp, ip], ctypes.c_int),
         "lbm_get_mean_density": ([vp, dp], ctypes.c_int),
+        "lbm_compute_error": ([vp, dp], ctypes.c_int),
         "lbm_get_state": ([vp, dp, dp, dp], ctypes.c_int),
         "lbm_set_state": ([vp, ctypes.c_int64, dp, dp, ctypes.c_int32, dp], ctypes.c_int),
         "lbm_get_status": ([vp], ctypes.c_int),
@@ -347,6 +348,13 @@ class Simulation:
     def mean_density(self) -> float:
         v = ctypes.c_double()
         self._check(self.lib.lbm_get_mean_density(self._h, ctypes.byref(v)), "lbm_get_mean_density")
+        return v.value
+
+    def compute_error(self) -> float:
+        """COMPUTEERROR (C1:1592-1612): relative velocity change since the
+        previous call (since the initial state on the first call)."""
+        v = ctypes.c_double()
+        self._check(self.lib.lbm_compute_error(self._h, ctypes.byref(v)), "lbm_compute_error")
         return v.value
 
     def get_state(self):

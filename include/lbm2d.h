@@ -187,6 +187,13 @@ int lbm_series_record_len(lbm_sim* h, int32_t* len);
 /* Mean density SUM(RHO)/((NX+1)(NY+1)) of the current state (C1:318). */
 int lbm_get_mean_density(lbm_sim* h, double* avg);
 
+/* Convergence measure of COMPUTEERROR (C1:1592-1612), which the reference
+ * calls every 1000 steps (C1:321-325): ER = sqrt(sum |u - u0|^2 / sum |u|^2)
+ * over all nodes, u the corrected velocity of the current step and u0 the
+ * velocity of the previous call (zero before the first call, as U0 = UX
+ * after INITIALIZE, C1:154-155); the call then keeps u as the new u0. */
+int lbm_compute_error(lbm_sim* h, double* er);
+
 /* Checkpoint: the complete dynamic state of step KK, as the reference's
  * restart dump holds it (C1:351-379): f is 9*(NX+1)*(NY+1) doubles in the
  * F(0:8,0:NX,0:NY) order holding F after the boundary conditions of step KK;

@@ -41,6 +41,7 @@ struct oracle {
     int nx, ny, n1x, n1y;
     size_t nn;
     double *F, *FPOST, *FEQ, *G, *RHO, *UX, *UY, *OMEGA_BN, *STRESS;
+    double *U0, *V0;  /* COMPUTEERROR's previous velocity (allocated on first use) */
     int32_t* IMAGE;
     uint8_t* IS_PARTICLE;
     double omega, omega_mrt[Q];
@@ -639,6 +640,7 @@ void oracle_destroy(oracle* o) {
     free(o->disk);
     free(o->F); free(o->FPOST); free(o->FEQ); free(o->G); free(o->RHO); free(o->UX);
     free(o->UY); free(o->OMEGA_BN); free(o->STRESS); free(o->IMAGE); free(o->IS_PARTICLE);
+    free(o->U0); free(o->V0);
     free(o->series);
     free(o);
 }
@@ -789,3 +791,27 @@ int oracle_get_series(oracle* o, double* out, int32_t max_records, int32_t* nrec
 }
 
 double oracle_mean_density(oracle* o) { return o ? mean_density(o) : NAN; }
+
+/* ---- COMPUTEERROR, C1:1592-1612 (called at MOD(KK,1000)==0, C1:321-325):
+ * I outer, J inner; U0/V0 hold the velocity of the previous call and start
+ * as the INITIALIZE velocity, zero (C1:154-155). */
+int oracle_compute_error(oracle* o, double* er) {
+    if (!o || !er) return LBM_E_INVALID;
+    if (!o->U0) {
+        o->U0 = (double*)calloc(o->nn, sizeof(double));
+        o->V0 = (double*)calloc(o->nn, sizeof(double));
+        if (!o->U0 || !o->V0) return LBM_E_NOMEM;
+    }
+    double err1 = 0.0, err2 = 0.0;
+    for (int i = 0; i <= o->nx; ++i)
+        for (int j = 0; j <= o->ny; ++j) {
+            const size_t n = IDX(o, i, j);
+            err1 = err1 + ((o->UX[n] - o->U0[n]) * (o->UX[n] - o->U0[n]) +
+                           (o->UY[n] - o->V0[n]) * (o->UY[n] - o->V0[n]));
+            err2 = err2 + (o->UX[n] * o->UX[n] + o->UY[n] * o->UY[n]);
+            o->U0[n] = o->UX[n];
+            o->V0[n] = o->UY[n];
+        }
+    *er = sqrt(err1 / err2);
+    return LBM_OK;
+}

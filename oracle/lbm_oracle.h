@@ -59,6 +59,8 @@ int  oracle_get_next_post_collision(oracle* o, double* out, double* omega_out);
 int  oracle_get_series(oracle* o, double* out, int32_t max_records, int32_t* nrec);
 int  oracle_series_record_len(const oracle* o);
 double oracle_mean_density(oracle* o);
+/* COMPUTEERROR: ||u - u_prev|| / ||u||, then u_prev = u (C1:1592-1612) */
+int  oracle_compute_error(oracle* o, double* er);
 /* the reference's full particle state incl. VP_OLD (np*LBM_STATE_PER) */
 int  oracle_get_state_particles(oracle* o, double* out);
 

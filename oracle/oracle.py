@@ -63,6 +63,7 @@ def load():
             "oracle_series_record_len": ([vp], ctypes.c_int),
             "oracle_mean_density": ([vp], ctypes.c_double),
             "oracle_get_state_particles": ([vp, dp], ctypes.c_int),
+            "oracle_compute_error": ([vp, dp], ctypes.c_int),
         }
         for name, (args, res) in sigs.items():
             fn = getattr(lib, name)
@@ -166,3 +167,10 @@ class Oracle:
 
     def mean_density(self):
         return float(self.lib.oracle_mean_density(self._h))
+
+    def compute_error(self):
+        er = ctypes.c_double()
+        rc = self.lib.oracle_compute_error(self._h, ctypes.byref(er))
+        if rc != 0:
+            raise _lbm.LbmError(rc, "oracle_compute_error")
+        return er.value

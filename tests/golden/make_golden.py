@@ -19,6 +19,8 @@ named; only PARAMETERs and the particle input file are replaced):
              disk at its coded start (12, 18)), 30 steps: half-way
              bounce-back, Papanastasiou viscosity with the node-to-node omega
              chain, rate set q(omega), angle integration
+  c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
+             the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
   c3_multi   3_MultiParticle_Sedimentation (C3), NX=48 NY=72, N_PARTICLE=3
              (D = L_C = 16), 20 steps: pair repulsion including the stale
              D_PW contact test.  The STOP at C3:202, which ends the shipped
@@ -53,6 +55,9 @@ CASES = {
     "c1_walls": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
                      overrides={"NX": "24", "NY": "40", "TIME_MAX": "20"},
                      particles="19.02\t4.98\t8\t1.25", steps=20),
+    "c1_error": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
+                     overrides={"NX": "16", "NY": "24", "TIME_MAX": "2000"},
+                     particles="8\t14\t6\t1.25", steps=2000),
     "c6_bingham": dict(file="6_FreeFall_YieldStress/D2Q9_BinghamSediment_Validated_20191127.f90",
                        overrides={"NX": "24", "NY": "60", "TIME_MAX": "30"},
                        particles=None, steps=30),

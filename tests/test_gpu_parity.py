@@ -216,3 +216,21 @@ def test_c1_matches_reference_golden(pkg, cases, name, centre, precision, rtol):
         close64(gp[:, 9:11], fc, rtol, "wall repulsion", scale=max(np.max(np.abs(fc)), 1e-300))
     finally:
         sim.close()
+
+
+@pytest.mark.parametrize("precision,rtol", [(0, 1e-10), (1, 2e-4)])
+def test_compute_error_matches_oracle(pkg, cases, precision, rtol):
+    """lbm_compute_error against the oracle's COMPUTEERROR, two calls in a
+    row (the second measures the change since the first)."""
+    p = cases.shipped_c1(48, 72, 12.0)
+    p.precision = precision
+    pin = cases.pin_array([[24.0, 50.0]], 12.0, 1.25)
+    sim, ref = pair(pkg, p, pin, 30)
+    try:
+        assert sim.compute_error() == pytest.approx(ref.compute_error(), rel=rtol)
+        sim.step(25)
+        ref.step(25)
+        assert sim.compute_error() == pytest.approx(ref.compute_error(), rel=rtol)
+    finally:
+        sim.close()
+        ref.close()

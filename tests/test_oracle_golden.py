@@ -98,3 +98,22 @@ def test_goldens_cover_the_branches_they_claim():
     om = c6["OMEGA_BN"]
     assert om.min() < om.max()                                # Bingham omega varies
     assert np.any(c6["DISK_ANGLE"] != 0) or np.any(c6["DISK_VELOCITY"][:, 2] != 0)
+
+
+def test_oracle_compute_error_matches_reference(cases):
+    """COMPUTEERROR (C1:1592-1612) as the reference evaluates it every 1000
+    steps (unit 7 of its run): ER at steps 1000 and 2000, and the state."""
+    g = _load("c1_error")
+    p = cases.shipped_c1(16, 24, 6.0)
+    o = Oracle(p)
+    try:
+        o.set_particles(cases.pin_array([[8.0, 14.0]], 6.0, 1.25))
+        ers = []
+        for _ in range(2):
+            o.step(1000)
+            ers.append([float(o.kk), o.compute_error()])
+        _exact(np.array(ers), g["UNIT7"], "ER history")
+        _exact(o.field("ux").T, g["UX"], "UX")
+        _exact(o.particles()[:, 0:2], g["DISK_CENTER"], "CENTER")
+    finally:
+        o.close()
