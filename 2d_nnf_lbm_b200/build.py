@@ -74,6 +74,18 @@ def build(verbose: bool = False, force: bool = False, out: str = OUT,
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    # the C++ driver that mirrors the reference's MAIN on the C ABI
+    drv_src = os.path.join(HERE, "driver", "lbm_main.cpp")
+    drv = os.path.join(os.path.dirname(out), "lbm_main")
+    if os.path.exists(drv_src) and (force or _stale(drv, [drv_src, out, *headers])):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"),
+               drv_src, "-L", os.path.dirname(out), "-l:" + os.path.basename(out),
+               "-Wl,-rpath,$ORIGIN", "-o", drv]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("driver build failed")
     with open(os.path.join(build_dir, "ptxas.log"), "a") as fh:
         fh.write("".join(logs))
     if verbose:
