@@ -48,6 +48,9 @@ struct lbm_sim {
   int* tile_count = nullptr;
   int* tile_list = nullptr;
   int* tile_cur = nullptr;
+  int* tile_order = nullptr;  // [2][ntiles]
+  int* n_unlisted = nullptr;  // [2]
+  int* work_ctr = nullptr;    // [2]
   int tile_cap = MAX_TILE_CAND;
   int* nbr = nullptr;
   int* nbr_count = nullptr;
@@ -165,6 +168,9 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
   a.tile_cur = h->tile_cur;
+  a.tile_order = h->tile_order;
+  a.n_unlisted = h->n_unlisted;
+  a.work_ctr = h->work_ctr;
   a.tile_cap = h->tile_cap;
   a.ntiles = h->g.ltx * h->g.lty;
   a.facc = h->facc;
@@ -185,6 +191,9 @@ ParticleArgs particle_args(lbm_sim* h) {
   a.tile_count = h->tile_count;
   a.tile_list = h->tile_list;
   a.tile_cur = h->tile_cur;
+  a.tile_order = h->tile_order;
+  a.n_unlisted = h->n_unlisted;
+  a.work_ctr = h->work_ctr;
   a.tile_cap = h->tile_cap;
   a.ntiles = h->g.ltx * h->g.lty;
   a.nbx = h->g.ltx;
@@ -349,7 +358,10 @@ void particle_record(const lbm_params& p, double* P, double x, double y, double 
 int launch_tiles(lbm_sim* h) {
   ParticleArgs pa = particle_args(h);
   CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.ltx * h->g.lty, h->stream));
+  CK(cudaMemsetAsync(h->work_ctr, 0, 2 * sizeof(int), h->stream));
   CK(launch_tiles_only(pa, h->stream));
+  CK(launch_tile_order(pa, 0, h->stream));
+  CK(launch_tile_order(pa, 1, h->stream));
   return LBM_OK;
 }
 
@@ -401,7 +413,8 @@ void to_pitched(const double* src_dense, std::vector<unsigned char>& buf, const 
         const size_t o = (size_t)j * n1x + i;
         double v = aos9 ? src_dense[o * 9 + k] : src_dense[(size_t)k * n1x * n1y + o];
         if (shift) v -= w[k] * h->p.rho0;
-        d[(size_t)k * h->g.plane + (size_t)j * h->g.pitch + i] = (T)v;
+        const int pl = planes == 9 ? plane_of(k) : k;  // population planes (plane_of)
+        d[(size_t)pl * h->g.plane + (size_t)j * h->g.pitch + i] = (T)v;
       }
 }
 
@@ -440,7 +453,8 @@ cudaError_t record_event(lbm_sim* h) {
 }
 
 // Tensor maps over the population buffers, 3-D (x = pitch, y = NY+1,
-// z = 9 planes), box = one step-kernel tile of one plane.  The encoder comes
+// z = 9 planes), box = one step-kernel tile of the three planes that share a
+// row shift (plane_of).  The encoder comes
 // from the driver through the runtime, so no link against libcuda is needed.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -459,7 +473,7 @@ int make_tensor_maps(lbm_sim* h) {
   const cuuint64_t strides[2] = {(cuuint64_t)h->g.pitch * h->esz,
                                  (cuuint64_t)h->g.plane * h->esz};
   const cuuint32_t box[3] = {(cuuint32_t)step_box_width((int)h->esz),
-                             (cuuint32_t)step_box_rows((int)h->esz), 1};
+                             (cuuint32_t)step_box_rows((int)h->esz), 3};
   const cuuint32_t es[3] = {1, 1, 1};
   for (int b = 0; b < 2; ++b) {
     CUresult r = enc(&h->tm[b],
@@ -482,6 +496,7 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->rec);
   dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
   dfree(h->tile_count); dfree(h->tile_list); dfree(h->tile_cur); dfree(h->pair_rebuild);
+  dfree(h->tile_order); dfree(h->n_unlisted); dfree(h->work_ctr);
   dfree(h->rec_slot);
   dfree(h->mass_acc);
   dfree(h->d_kk); dfree(h->stale_dpw);
@@ -710,6 +725,10 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);
   if ((rc = dalloc(&h->tile_list, (size_t)2 * ntiles * h->tile_cap))) return fail(rc);
   if ((rc = dalloc(&h->tile_cur, 2))) return fail(rc);
+  if ((rc = dalloc(&h->tile_order, (size_t)2 * ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->n_unlisted, 2))) return fail(rc);
+  if ((rc = dalloc(&h->work_ctr, 2))) return fail(rc);
+  cudaMemsetAsync(h->work_ctr, 0, 2 * sizeof(int), h->stream);
   if ((rc = dalloc(&h->pair_rebuild, 1))) return fail(rc);
   if ((rc = dalloc(&h->rec_slot, 1))) return fail(rc);
   cudaMemsetAsync(h->rec_slot, 0xff, sizeof(int), h->stream);
@@ -725,6 +744,12 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   const double inf = INFINITY;
   cudaMemcpyAsync(h->stale_dpw, &inf, sizeof(double), cudaMemcpyHostToDevice, h->stream);
   if ((rc = setup_particle_buffers(h, 0, 0.0))) return fail(rc);
+  {  // empty lists: the tile queue order of both buffers
+    ParticleArgs pa = particle_args(h);
+    if (launch_tile_order(pa, 0, h->stream) != cudaSuccess ||
+        launch_tile_order(pa, 1, h->stream) != cudaSuccess)
+      return fail(LBM_E_CUDA);
+  }
   // f*(1) = collision of step 1 applied to INITIALIZE's state (C1:151, C1:296)
   h->cur = 0;
   LatticeArgs a = lattice_args(h);

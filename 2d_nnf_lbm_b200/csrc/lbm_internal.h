@@ -73,6 +73,14 @@ struct Geometry {
   int ltx, lty;      // list tiles
 };
 
+// Population k lives in plane plane_of(k) of a population buffer.  The planes
+// are grouped by the row shift c_y of the pull (0: k=0,1,3; +1: k=2,5,6;
+// -1: k=4,7,8), so one 3-D TMA box of depth 3 fetches the three planes that
+// share a row offset.
+__host__ __device__ constexpr int plane_of(int k) {
+  return k == 2 ? 3 : k == 3 ? 2 : k == 4 ? 6 : k == 5 ? 4 : k == 6 ? 5 : k;
+}
+
 struct Model {
   int bc;            // LBM_BC_*
   int bingham;       // 1: Papanastasiou
@@ -96,6 +104,9 @@ struct ParticleArgs {
   int* tile_count;           // [2][ntiles]
   int* tile_list;            // [2][ntiles][tile_cap]
   int* tile_cur;             // [2]: list buffer valid for step k at [k&1]
+  int* tile_order;           // [2][ntiles]: list tiles, those without disks first
+  int* n_unlisted;           // [2]: how many list tiles have no disk
+  int* work_ctr;             // [2]: step-kernel tile queue of step k at [k&1]
   int tile_cap;
   int ntiles, nbx;
   int* nbr;                  // [MAX_NEIGH][npad]
@@ -133,6 +144,9 @@ struct LatticeArgs {
   const int* tile_count; // [2][ntiles]
   const int* tile_list;
   const int* tile_cur;   // [2]: list buffer valid for step k at [k&1]
+  const int* tile_order; // [2][ntiles]: list tiles, those without disks first
+  const int* n_unlisted; // [2]
+  int* work_ctr;         // [2]: tile queue of step k at [k&1], zero at the start
   int tile_cap;
   int ntiles;
   unsigned long long* facc;  // [6][npad]
@@ -166,6 +180,8 @@ inline int step_box_rows(int esz) { return 512 / (esz == 8 ? 64 : 128); }
 
 // Particle kernel (lbm_particles.cu).
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
+// tile_order / n_unlisted of list buffer buf from its counts.
+cudaError_t launch_tile_order(const ParticleArgs& a, int buf, cudaStream_t s);
 // Tile lists (into buffer 0) and a pair-list rebuild request, after
 // set_particles / set_state.
 cudaError_t launch_tiles_only(const ParticleArgs& a, cudaStream_t s);

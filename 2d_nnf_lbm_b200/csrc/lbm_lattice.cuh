@@ -331,18 +331,19 @@ __device__ __forceinline__ void pull_bc(const T* __restrict__ src, const Geometr
   const long long n = (long long)j * g.pitch + i;
   const int pt = g.pitch;
   const bool L = (i == 0), R = (i == g.nx), B = (j == 0), U = (j == g.ny);
-  f[0] = src[n];
-  f[1] = !L ? src[P + n - 1] : src[P + n];
-  f[2] = !B ? src[2 * P + n - pt] : src[2 * P + n];
-  f[3] = !R ? src[3 * P + n + 1] : src[3 * P + n];
-  f[4] = !U ? src[4 * P + n + pt] : src[4 * P + n];
-  f[5] = (!L && !B) ? src[5 * P + n - pt - 1] : src[5 * P + n];
-  f[6] = (!R && !B) ? src[6 * P + n - pt + 1] : src[6 * P + n];
-  f[7] = (!R && !U) ? src[7 * P + n + pt + 1] : src[7 * P + n];
-  f[8] = (!L && !U) ? src[8 * P + n + pt - 1] : src[8 * P + n];
+  const T* s0 = src + n;
+  f[0] = s0[0];
+  f[1] = !L ? s0[plane_of(1) * P - 1] : s0[plane_of(1) * P];
+  f[2] = !B ? s0[plane_of(2) * P - pt] : s0[plane_of(2) * P];
+  f[3] = !R ? s0[plane_of(3) * P + 1] : s0[plane_of(3) * P];
+  f[4] = !U ? s0[plane_of(4) * P + pt] : s0[plane_of(4) * P];
+  f[5] = (!L && !B) ? s0[plane_of(5) * P - pt - 1] : s0[plane_of(5) * P];
+  f[6] = (!R && !B) ? s0[plane_of(6) * P - pt + 1] : s0[plane_of(6) * P];
+  f[7] = (!R && !U) ? s0[plane_of(7) * P + pt + 1] : s0[plane_of(7) * P];
+  f[8] = (!L && !U) ? s0[plane_of(8) * P + pt - 1] : s0[plane_of(8) * P];
   if (!(L || R || B || U)) return;
   // own post-collision populations F_POST(k,i,j)
-#define FPOST(k) src[(k) * P + n]
+#define FPOST(k) src[plane_of(k) * P + n]
   if ((L || R) && (B || U)) {
     // corners: half-way bounce-back of 3 of the 5 unknowns (C1:1390-1414)
     if (L && B) { f[1] = FPOST(3); f[5] = FPOST(7); f[2] = FPOST(4); }
@@ -383,15 +384,16 @@ __device__ __forceinline__ void pull_interior(const T* __restrict__ src, const G
                                               long long n, T* f) {
   const long long P = g.plane;
   const int pt = g.pitch;
-  f[0] = src[n];
-  f[1] = src[P + n - 1];
-  f[2] = src[2 * P + n - pt];
-  f[3] = src[3 * P + n + 1];
-  f[4] = src[4 * P + n + pt];
-  f[5] = src[5 * P + n - pt - 1];
-  f[6] = src[6 * P + n - pt + 1];
-  f[7] = src[7 * P + n + pt + 1];
-  f[8] = src[8 * P + n + pt - 1];
+  const T* s0 = src + n;
+  f[0] = s0[0];
+  f[1] = s0[plane_of(1) * P - 1];
+  f[2] = s0[plane_of(2) * P - pt];
+  f[3] = s0[plane_of(3) * P + 1];
+  f[4] = s0[plane_of(4) * P + pt];
+  f[5] = s0[plane_of(5) * P - pt - 1];
+  f[6] = s0[plane_of(6) * P - pt + 1];
+  f[7] = s0[plane_of(7) * P + pt + 1];
+  f[8] = s0[plane_of(8) * P + pt - 1];
 }
 
 // ---------------------------------------------------------------------------
@@ -497,7 +499,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
       for (int k = 0; k < 9; ++k) f[k] = F64 ? (T)feq[k] : (T)(feq[k] - wexact(k) * m.rho0);
     } else if (MODE == MODE_RESTART || (MODE == MODE_OUTPUT && a.src_post_bc)) {
 #pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = src[k * g.plane + n];
+      for (int k = 0; k < 9; ++k) f[k] = src[plane_of(k) * g.plane + n];
     } else {
       const bool interior = blockIdx.x > 0 && blockIdx.y > 0 &&
                             (int)(blockIdx.x + 1) * TX <= g.nx &&
@@ -672,7 +674,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
   }
   T* __restrict__ dst = static_cast<T*>(a.dst);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) dst[k * g.plane + n] = f[k];
+  for (int k = 0; k < 9; ++k) dst[plane_of(k) * g.plane + n] = f[k];
   if (m.bingham) static_cast<T*>(a.om_dst)[n] = (T)no.omega;
   if (m.record_stress) {
     const int slot = (int)((kk + 1) & 1);
@@ -702,7 +704,6 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
 // zero-filled by the TMA unit; the nodes on the lattice edge gather their
 // populations from global memory with the boundary conditions instead.
 constexpr int STEP_CONSUMERS = 512;              // consumer threads (16 warps)
-constexpr int STEP_MASKS = 64;  // 32-tile masks per CTA: up to 2048 tiles split by pass
 constexpr int STEP_TPB = STEP_CONSUMERS + 32;    // + one producer warp
 
 template <class T>
@@ -721,6 +722,8 @@ struct Stage {
 constexpr int NSTAGE = LBM_STEP_STAGES;
 
 // Particles touching one tile, staged by the producer warp (one per stage).
+// One lane per candidate: the consumers cull them with a warp ballot.
+static_assert(MAX_TILE_CAND <= 32, "one candidate per lane");
 struct TileCand {
   double px[MAX_TILE_CAND], py[MAX_TILE_CAND], pr[MAX_TILE_CAND];
   double pu[MAX_TILE_CAND], pv[MAX_TILE_CAND], pw[MAX_TILE_CAND];
@@ -759,14 +762,15 @@ __device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, ui
   using ST = Stage<T>;
   const int x = bx * ST::TW - ST::H;  // a multiple of H: 16-byte aligned
   const int y0 = by * ST::TR;
+  // three boxes of three planes: row shifts c_y = 0, +1, -1 (plane_of)
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const int cy = (k == 2 || k == 5 || k == 6) ? 1 : ((k == 4 || k == 7 || k == 8) ? -1 : 0);
-    const uint32_t d = dst + (uint32_t)(k * ST::PLANE * (int)sizeof(T));
+  for (int gq = 0; gq < 3; ++gq) {
+    const int cy = gq == 0 ? 0 : (gq == 1 ? 1 : -1);
+    const uint32_t d = dst + (uint32_t)(3 * gq * ST::PLANE * (int)sizeof(T));
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
         "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(d),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y0 - cy), "r"(k), "r"(mbar)
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y0 - cy), "r"(3 * gq), "r"(mbar)
         : "memory");
   }
 }
@@ -843,94 +847,142 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  // every CTA is resident: the next step's particle kernel may be scheduled
+  // (it waits for this grid before it touches anything)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
-  __shared__ unsigned s_mask[STEP_MASKS];
   if (warp == STEP_CONSUMERS / 32) {
     // ================= producer warp =====================================
-    // Pass 0: tiles that no disk can reach by the lists of the previous step
-    // (a disk moves less than the Verlet skin between list builds); they need
-    // nothing from this step's particle kernel, which may still be running.
-    // Pass 1: after griddepcontrol.wait, the tiles that list disks, with the
-    // disks' state of this step and the lists valid for it.
+    // Tiles come from one queue shared by all CTAs (work_ctr[step & 1]): the
+    // step tiles of the list tiles in tile_order of the previous step's list
+    // buffer, the tiles no disk can reach first (a disk moves less than the
+    // Verlet skin between list builds).  Those need nothing from this step's
+    // particle kernel, which may still be running; the first tile that lists
+    // disks waits for it (griddepcontrol.wait), and by then every
+    // particle-free tile has been handed out.  Taking tiles one at a time
+    // from the queue keeps the CTAs finishing together.
     int bo = 0;
     if (lane == 0) bo = a.tile_cur[(a.step - 1) & 1];
     const int buf_old = __shfl_sync(0xffffffffu, bo, 0);
-    // which of this CTA's tiles list disks: one bit per tile, 32 tiles per
-    // load across the lanes (n-th tile of the CTA: t = blockIdx.x + n*gridDim.x)
-    const int nmine = (ntx * nty - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-    const int nch = (nmine + 31) / 32;
-    const bool split = nch <= STEP_MASKS;  // else every tile waits for the particle kernel
-    if (split) {
-      for (int ch = 0; ch < nch; ++ch) {
-        const int nn = ch * 32 + lane;
-        bool listed = false;
-        if (nn < nmine) {
-          const int t = (int)blockIdx.x + nn * (int)gridDim.x;
-          const int by = t / ntx, bx = t - by * ntx;
-          const int lt = ((by * ST::TR) / LTY) * g.ltx + (bx * ST::TW) / LTX;
-          listed = a.tile_count[(long long)buf_old * a.ntiles + lt] > 0;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, listed);
-        if (lane == 0) s_mask[ch] = m;
-      }
-      __syncwarp();
-    }
+    int nu = 0;
+    if (lane == 0) nu = a.n_unlisted[buf_old];
+    const int* order = a.tile_order + (long long)buf_old * a.ntiles;
+    int* ctr = a.work_ctr + (a.step & 1);
+    constexpr int SX = LTX / ST::TW, SY = LTY / ST::TR, S = SX * SY;  // step tiles per list tile
+    const int Q = S * a.ntiles;
     int buf = -1;
+    bool waited = false;
     int sidx = 0;
     uint32_t epar = 0;  // per-stage parity of the next "empty" completion
     uint32_t fpar = 0;  // per-stage parity of the next "full" completion
     int n = 0;          // tiles issued
     bool alive = true;
-    for (int pass = split ? 0 : 1; pass < 2 && alive; ++pass) {
-      if (pass == 1) {
+
+    // One queue entry: false once the queue is exhausted or the consumers
+    // gave up.
+    auto issue = [&](int t, int L) -> bool {
+      if (t >= Q) return false;
+      if ((unsigned)L >= (unsigned)a.ntiles) {  // never for a built order; no stray tile
+        if (lane == 0) atomicOr(a.status, ST_OVERFLOW);
+        return true;
+      }
+      const int sub = t % S, ly = L / g.ltx, lx = L - ly * g.ltx;
+      const int bx = lx * SX + sub % SX, by = ly * SY + sub / SX;
+      if (bx >= ntx || by >= nty) return true;  // past the lattice: no slot
+      const bool listed = t / S >= __shfl_sync(0xffffffffu, nu, 0);
+      if (listed && !waited) {
         asm volatile("griddepcontrol.wait;" ::: "memory");
         int bn = 0;
         if (lane == 0) bn = a.tile_cur[a.step & 1];
         buf = __shfl_sync(0xffffffffu, bn, 0);
+        waited = true;
       }
-      for (int ch = 0; ch < nch && alive; ++ch) {
-        const unsigned valid = ch * 32 + 32 <= nmine ? 0xffffffffu : ((1u << (nmine - ch * 32)) - 1u);
-        unsigned todo = !split ? valid : (pass == 0 ? ~s_mask[ch] & valid : s_mask[ch]);
-        while (todo) {
-        const int bit = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int t = (int)blockIdx.x + (ch * 32 + bit) * (int)gridDim.x;
-        const int by = t / ntx, bx = t - by * ntx;
-        if (n >= NSTAGE) {
-          bool ok = true;
-          if (lane == 0) {
-            ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
-            if (!ok) atomicOr(a.status, ST_TIMEOUT);
-          }
-          epar ^= 1u << sidx;
-          ok = __shfl_sync(0xffffffffu, ok, 0);
-          if (!ok) {
-            // consumers gave up: let the boxes already in flight land (bounded)
-            if (lane == 0) {
-              for (int st = 0; st < NSTAGE; ++st)
-                mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
-            }
-            alive = false;
-            break;
-          }
-        }
-        stage_candidates<T>(a, bx, by, buf, cands[sidx], lane);
-        __syncwarp();
+      if (n >= NSTAGE) {
+        bool ok = true;
         if (lane == 0) {
-          // boxes reaching past the lattice are filled with zeros; they still
-          // deliver their full byte count
-          const uint32_t fb = full0 + 8 * sidx;
+          ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+          if (!ok) atomicOr(a.status, ST_TIMEOUT);
+        }
+        epar ^= 1u << sidx;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          // consumers gave up: let the boxes already in flight land (bounded)
+          if (lane == 0) {
+            for (int st = 0; st < NSTAGE; ++st)
+              mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
+          }
+          alive = false;
+          return false;
+        }
+      }
+      stage_candidates<T>(a, bx, by, listed ? buf : -1, cands[sidx], lane);
+      __syncwarp();
+      if (lane == 0) {
+        const uint32_t fb = full0 + 8 * sidx;
+        if (bx * ST::TW >= g.nx) {
+          // every node of the tile is on the right edge (the last column of
+          // an NX that is a multiple of TW) and gathers from global memory:
+          // no stage data, the slot is released at once
+          mbar_arrive(fb);
+        } else {
+          // boxes reaching past the lattice are filled with zeros; they
+          // still deliver their full byte count
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
                        "r"((uint32_t)ST::BYTES)
                        : "memory");
           tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
         }
-        fpar ^= 1u << sidx;
-        sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
-        ++n;
+      }
+      fpar ^= 1u << sidx;
+      sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
+      ++n;
+      return true;
+    };
+
+    // Lane 0 runs the queue with three (index, list tile) register pairs
+    // that rotate through "take" (atomicAdd issued), "look up" (order load
+    // issued) and "issue", so neither latency is waited for while the ring
+    // has work.
+    int t0 = 0, L0 = 0, t1 = 0, L1 = 0, t2 = 0, L2 = 0;
+    if (lane == 0) {
+      t0 = atomicAdd(ctr, 2);
+      t1 = t0 + 1;
+      L0 = t0 < Q ? order[t0 / S] : 0;
+    }
+    for (;;) {
+      if (lane == 0) {
+        L1 = t1 < Q ? order[t1 / S] : 0;
+        t2 = atomicAdd(ctr, 1);
+      }
+      if (!issue(__shfl_sync(0xffffffffu, t0, 0), __shfl_sync(0xffffffffu, L0, 0))) break;
+      if (lane == 0) {
+        L2 = t2 < Q ? order[t2 / S] : 0;
+        t0 = atomicAdd(ctr, 1);
+      }
+      if (!issue(__shfl_sync(0xffffffffu, t1, 0), __shfl_sync(0xffffffffu, L1, 0))) break;
+      if (lane == 0) {
+        L0 = t0 < Q ? order[t0 / S] : 0;
+        t1 = atomicAdd(ctr, 1);
+      }
+      if (!issue(__shfl_sync(0xffffffffu, t2, 0), __shfl_sync(0xffffffffu, L2, 0))) break;
+    }
+    if (alive) {
+      // end marker: a stage whose tile column is -1
+      bool ok = true;
+      if (lane == 0) {
+        if (n >= NSTAGE) {
+          ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+          if (!ok) atomicOr(a.status, ST_TIMEOUT);
+        }
+        if (ok) {
+          cands[sidx].bx = -1;
+          mbar_arrive(full0 + 8 * sidx);
         }
       }
     }
+    // this grid completes only after this step's particle kernel, so the
+    // next one (waiting on this grid) never overlaps it
+    if (!waited) asm volatile("griddepcontrol.wait;" ::: "memory");
     return;
   }
 
@@ -942,17 +994,17 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
   T* __restrict__ dst = static_cast<T*>(a.dst);
   const long long P = g.plane;
   const int pt = g.pitch;
-  const int nmine = (ntx * nty - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
 
-  for (int n = 0; n < nmine; ++n, sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
+  for (;; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
     if (!mbar_wait(full0 + 8 * sidx, (fpar >> sidx) & 1u, WAIT)) {
       if (lane == 0) atomicOr(a.status, ST_TIMEOUT);
       return;
     }
     fpar ^= 1u << sidx;
     const int bx = cands[sidx].bx, by = cands[sidx].by;  // set by the producer
+    if (bx < 0) break;  // the producer's end marker
     const int i = bx * ST::TW + tc;
     const int j = by * ST::TR + tr;
     const long long nd = (long long)j * pt + i;
@@ -973,15 +1025,17 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
     T f[9];
     if (!edge) {
       const T* q = stage + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
+      // planes in plane_of order; the row shift is in the box, the column
+      // shift -c_x is applied here
       f[0] = q[0];
-      f[1] = q[ST::PLANE - 1];
-      f[2] = q[2 * ST::PLANE];
-      f[3] = q[3 * ST::PLANE + 1];
-      f[4] = q[4 * ST::PLANE];
-      f[5] = q[5 * ST::PLANE - 1];
-      f[6] = q[6 * ST::PLANE + 1];
-      f[7] = q[7 * ST::PLANE + 1];
-      f[8] = q[8 * ST::PLANE - 1];
+      f[1] = q[plane_of(1) * ST::PLANE - 1];
+      f[2] = q[plane_of(2) * ST::PLANE];
+      f[3] = q[plane_of(3) * ST::PLANE + 1];
+      f[4] = q[plane_of(4) * ST::PLANE];
+      f[5] = q[plane_of(5) * ST::PLANE - 1];
+      f[6] = q[plane_of(6) * ST::PLANE + 1];
+      f[7] = q[plane_of(7) * ST::PLANE + 1];
+      f[8] = q[plane_of(8) * ST::PLANE - 1];
     } else if (act) {
       pull_bc<T>(src, g, m.bc, i, j, f);
     } else {
@@ -1019,8 +1073,26 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
     //      C1:500-507) and force sums ---------------------------------------
     T gx = (T)0, gy = (T)0;
     int gbest = -1;
-    const int ncand = C.n;
-    for (int c = 0; c < ncand; ++c) {
+    // Only the candidates whose disk reaches this warp's 32 nodes of row j
+    // are visited: for the others every node of the segment is at least
+    // R + zeta/2 + 1e-3 from the centre, so PHI is 0 there in either
+    // precision (rounding of the node distance is far below 1e-3) and the
+    // skipped iterations would add nothing.
+    unsigned near = 0;
+    {
+      bool nr = false;
+      if (lane < C.n) {  // the warp's nodes: columns i - lane .. i - lane + 31
+        const double dl = (double)(i - lane) - C.px[lane], dr = dl + 31.0;
+        const double dx = dl > 0.0 ? dl : (dr < 0.0 ? -dr : 0.0);
+        const double dy = (double)j - C.py[lane];
+        const double reach = C.pr[lane] + 0.5 * m.zeta + 1e-3;
+        nr = dx * dx + dy * dy < reach * reach;
+      }
+      near = __ballot_sync(0xffffffffu, nr);
+    }
+    while (near) {
+      const int c = __ffs(near) - 1;
+      near &= near - 1;
       double fx = 0.0, fy = 0.0, tz = 0.0;
       bool hit = false;
       if (act) {
@@ -1121,7 +1193,7 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
       for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) dst[k * P + nd] = f[k];
+    for (int k = 0; k < 9; ++k) dst[plane_of(k) * P + nd] = f[k];
     if (m.bingham) static_cast<T*>(a.om_dst)[nd] = (T)no.omega;
     if (m.record_stress) {
       const int slot = (kpar + 1) & 1;

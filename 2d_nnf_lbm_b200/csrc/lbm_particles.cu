@@ -96,6 +96,55 @@ __device__ __forceinline__ void insert_tiles(const ParticleArgs& a, int p, doubl
   }
 }
 
+// Order of the list tiles of buffer buf for the step kernel's tile queue:
+// the tiles without disks first, then those with, each group in index order;
+// n_unlisted[buf] = size of the first group.  Run by one block.
+__device__ void build_tile_order(const ParticleArgs& a, int buf) {
+  __shared__ int s_w[PBLK / 32];
+  __shared__ int s_base[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x / 32;
+  const int* cnt = a.tile_count + (long long)buf * a.ntiles;
+  int* ord = a.tile_order + (long long)buf * a.ntiles;
+  int nu = 0;
+  for (int t = tid; t < a.ntiles; t += blockDim.x) nu += cnt[t] == 0 ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) nu += __shfl_xor_sync(0xffffffffu, nu, o);
+  if (lane == 0) s_w[warp] = nu;
+  if (tid == 0) s_base[0] = s_base[1] = 0;
+  __syncthreads();
+  int total_u = 0;
+  for (int w = 0; w < nw; ++w) total_u += s_w[w];
+  __syncthreads();
+  for (int c0 = 0; c0 < a.ntiles; c0 += blockDim.x) {
+    const int t = c0 + tid;
+    const bool in = t < a.ntiles;
+    const bool un = in && cnt[t] == 0;
+    // counts packed as unlisted | listed << 16 (at most 1024 per chunk)
+    const int v = (un ? 1 : 0) | ((in && !un) ? 1 << 16 : 0);
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    int before = 0, chunk = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) before += s_w[w];
+      chunk += s_w[w];
+    }
+    const int ex = before + inc - v;
+    if (un) ord[s_base[0] + (ex & 0xffff)] = t;
+    else if (in) ord[total_u + s_base[1] + (ex >> 16)] = t;
+    __syncthreads();
+    if (tid == 0) {
+      s_base[0] += chunk & 0xffff;
+      s_base[1] += chunk >> 16;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) a.n_unlisted[buf] = total_u;
+}
+
 __device__ __forceinline__ int cell_key(const ParticleArgs& a, double x, double y) {
   const int cx = clampi((int)floor(x / a.cell_size), 0, a.ncx - 1);
   const int cy = clampi((int)floor(y / a.cell_size), 0, a.ncy - 1);
@@ -197,7 +246,11 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
   __shared__ long long s_kk;
   __shared__ int s_pairs, s_tiles;
   const int tid = threadIdx.x;
-  // the lattice kernel of this step may start its particle-free tiles now
+  // Launched as a programmatic dependent of the previous step's lattice
+  // kernel: resident early, it waits here for that kernel (whose force sums
+  // it decodes and whose particle reads must end before the update below).
+  // Then the lattice kernel of this step may start its particle-free tiles.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (tid == 0) {
@@ -206,6 +259,9 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     *a.kk = k1;
     s_pairs = *a.pair_rebuild;
     s_tiles = 0;
+    // the tile queue of the next step (its last user, the step kernel of
+    // step k1 - 1, has completed)
+    a.work_ctr[(k1 + 1) & 1] = 0;
     const bool r = a.series != nullptr && a.series_every > 0 && (k1 % a.series_every) == 0;
     const long long slot = r ? (k1 / a.series_every - 1) % a.series_cap : -1;
     *a.rec_slot = (int)slot;  // read by the lattice kernel of this step
@@ -382,6 +438,8 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
       P[P_YT] = y;
     }
     __syncthreads();
+    build_tile_order(a, buf);
+    __syncthreads();
     if (tid == 0) a.tile_cur[s_kk & 1] = buf;
   }
 }
@@ -411,7 +469,25 @@ cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) attr[dev] = true;
   }
-  k_particles<<<1, PBLK, sizeof(PShared), s>>>(a);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(PBLK);
+  cfg.dynamicSmemBytes = sizeof(PShared);
+  cfg.stream = s;
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_particles, a);
+}
+
+__global__ void __launch_bounds__(PBLK) k_tile_order(const ParticleArgs a, int buf) {
+  build_tile_order(a, buf);
+}
+
+cudaError_t launch_tile_order(const ParticleArgs& a, int buf, cudaStream_t s) {
+  k_tile_order<<<1, PBLK, 0, s>>>(a, buf);
   return cudaGetLastError();
 }
 

@@ -234,3 +234,31 @@ def test_compute_error_matches_oracle(pkg, cases, precision, rtol):
     finally:
         sim.close()
         ref.close()
+
+
+@pytest.mark.parametrize("nx,precision", [(64, 0), (128, 0), (128, 1)])
+def test_wall_column_pass(pkg, cases, nx, precision):
+    """NX a multiple of the tile width: the wall column NX is taken by the last
+    warp of each tile row; a disk whose PHI ring reaches that column."""
+    p = cases.shipped_c1(nx, 48, 10.0)
+    p.gravity = -2e-4
+    p.wall_model = 2  # no wall repulsion: the disk stays on the wall column
+    pin = cases.pin_array([[nx - 5.2, 30.0]], 10.0, 1.5)
+    ref = Oracle(p)
+    ref.set_particles(pin)
+    sim = pkg.Simulation(p.copy(precision=precision))
+    sim.set_particles(pin)
+    sim.step(80)
+    ref.step(80)
+    assert ref.field("phi")[20:40, nx].max() > 0.0
+    if precision == 0:
+        compare_all(sim, ref)
+        return
+    g, r = sim.particles(), ref.particles()
+    for col in (0, 1, 3, 4):  # position (lu), velocity (against |u|)
+        scale = np.max(np.abs(r[:, [3, 4]])) if col in (3, 4) else 1.0
+        assert abs(g[0, col] - r[0, col]) <= 1e-4 * scale, (col, g[0, col], r[0, col])
+    for f in ("ux", "uy", "rho"):
+        a, b = sim.field(f), ref.field(f)
+        sc = np.max(np.abs(b - (1.0 if f == "rho" else 0.0)))
+        assert np.max(np.abs(a - b)) <= 1e-4 * max(sc, 1e-12), f
