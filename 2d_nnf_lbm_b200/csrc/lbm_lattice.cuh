@@ -725,7 +725,7 @@ constexpr int NSTAGE = LBM_STEP_STAGES;
 // One lane per candidate: the consumers cull them with a warp ballot.
 static_assert(MAX_TILE_CAND <= 32, "one candidate per lane");
 struct TileCand {
-  double px[MAX_TILE_CAND], py[MAX_TILE_CAND], pr[MAX_TILE_CAND];
+  double px[MAX_TILE_CAND], py[MAX_TILE_CAND], pd[MAX_TILE_CAND];  // pd: diameter
   double pu[MAX_TILE_CAND], pv[MAX_TILE_CAND], pw[MAX_TILE_CAND];
   int idx[MAX_TILE_CAND];
   int n;
@@ -775,51 +775,67 @@ __device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, ui
   }
 }
 
-// The producer warp stages the candidate particles of the list tile that
-// contains tile (bx, by).
-template <class T>
-__device__ __forceinline__ void stage_candidates(const LatticeArgs& a, int bx, int by, int buf,
-                                                 TileCand& C, int lane) {
-  using ST = Stage<T>;
+// Candidate particles of one tile.  No latency sits between a free ring
+// slot and its TMA issue: the count and the list row come in one round trip
+// before the slot is waited for (the whole row is read before the count is
+// known); after the TMA issue each lane copies its disk's state into the
+// stage with cp.async, tracked by the stage's "full" barrier, so the
+// producer never waits for it.
+struct CandList {
+  int n, idx;  // lane c: candidate c
+};
+
+__device__ __forceinline__ CandList cand_list(const LatticeArgs& a, int lt, int buf, int lane) {
+  CandList c{0, 0};
+  if (buf < 0) return c;  // a tile that no disk can reach
+  const long long tbase = (long long)buf * a.ntiles + lt;
+  c.n = a.tile_count[tbase];
+  if (lane < a.tile_cap) c.idx = a.tile_list[tbase * a.tile_cap + lane];
+  return c;
+}
+
+__device__ __forceinline__ void cp_async8(const void* smem, const void* gmem) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+}
+
+// Fill C for tile (bx, by) and make the second arrival on the stage's
+// "full" barrier fb once the copies have landed.
+__device__ __forceinline__ void cand_copy(const LatticeArgs& a, CandList c, int bx, int by,
+                                          TileCand& C, int lane, uint32_t fb) {
+  if (c.n > a.tile_cap) {
+    if (lane == 0) atomicOr(a.status, ST_OVERFLOW);
+    c.n = a.tile_cap;
+  }
+  if (lane < c.n) {
+    C.idx[lane] = c.idx;
+    const double* p = a.ps + c.idx;
+    const long long st = a.npad;
+    cp_async8(&C.px[lane], p + P_X * st);
+    cp_async8(&C.py[lane], p + P_Y * st);
+    cp_async8(&C.pd[lane], p + P_D * st);
+    cp_async8(&C.pu[lane], p + P_U * st);
+    cp_async8(&C.pv[lane], p + P_V * st);
+    cp_async8(&C.pw[lane], p + P_W * st);
+  }
+  // the barrier's phase waits for this lane's copies (pending count +1 now,
+  // -1 when they land); c.n is warp-uniform
+  if (c.n > 0) asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" ::"r"(fb) : "memory");
+  __syncwarp();
   if (lane == 0) {
     C.bx = bx;
     C.by = by;
+    C.n = c.n;
+    mbar_arrive(fb);
   }
-  if (buf < 0) {  // a tile that no disk can reach
-    if (lane == 0) C.n = 0;
-    return;
-  }
-  const int lt = ((by * ST::TR) / LTY) * a.g.ltx + (bx * ST::TW) / LTX;
-  const long long tbase = (long long)buf * a.ntiles + lt;
-  int c = a.tile_count[tbase];
-  if (c > a.tile_cap) {
-    if (lane == 0) atomicOr(a.status, ST_OVERFLOW);
-    c = a.tile_cap;
-  }
-  if (lane < c) {
-    const int pv = a.tile_list[tbase * a.tile_cap + lane];
-    const PRef p{const_cast<double*>(a.ps) + pv, a.npad};
-    C.idx[lane] = pv;
-    C.px[lane] = p[P_X];
-    C.py[lane] = p[P_Y];
-    C.pr[lane] = 0.5 * p[P_D];
-    C.pu[lane] = p[P_U];
-    C.pv[lane] = p[P_V];
-    C.pw[lane] = p[P_W];
-  }
-  if (lane == 0) C.n = c;
 }
 
 #ifndef LBM_STEP_MINB_F32
 #define LBM_STEP_MINB_F32 2
 #endif
-#ifndef LBM_STEP_MINB_F64
-#define LBM_STEP_MINB_F64 1
-#endif
 
 template <class T>
-__global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 : LBM_STEP_MINB_F32)
-    k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm) {
+__device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMap& tm) {
   constexpr bool F64 = sizeof(T) == 8;
   constexpr uint32_t WAIT = 1u << 20;
   using ST = Stage<T>;
@@ -839,7 +855,8 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
 
   if (tid == 0) {
     for (int st = 0; st < NSTAGE; ++st) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * st) : "memory");
+      // "full": the TMA boxes (expect_tx) and the candidates, two arrivals
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(full0 + 8 * st) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0 + 8 * st),
                    "r"(STEP_CONSUMERS / 32)
                    : "memory");
@@ -897,6 +914,8 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
         buf = __shfl_sync(0xffffffffu, bn, 0);
         waited = true;
       }
+      const CandList cl =
+          cand_list(a, ((by * ST::TR) / LTY) * g.ltx + (bx * ST::TW) / LTX, listed ? buf : -1, lane);
       if (n >= NSTAGE) {
         bool ok = true;
         if (lane == 0) {
@@ -915,14 +934,12 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
           return false;
         }
       }
-      stage_candidates<T>(a, bx, by, listed ? buf : -1, cands[sidx], lane);
-      __syncwarp();
+      const uint32_t fb = full0 + 8 * sidx;
       if (lane == 0) {
-        const uint32_t fb = full0 + 8 * sidx;
         if (bx * ST::TW >= g.nx) {
           // every node of the tile is on the right edge (the last column of
           // an NX that is a multiple of TW) and gathers from global memory:
-          // no stage data, the slot is released at once
+          // no stage data
           mbar_arrive(fb);
         } else {
           // boxes reaching past the lattice are filled with zeros; they
@@ -933,6 +950,8 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
           tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
         }
       }
+      // the candidates, while the boxes are in flight; second arrival
+      cand_copy(a, cl, bx, by, cands[sidx], lane, fb);
       fpar ^= 1u << sidx;
       sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
       ++n;
@@ -976,6 +995,7 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
         }
         if (ok) {
           cands[sidx].bx = -1;
+          mbar_arrive(full0 + 8 * sidx);  // both arrivals of the stage
           mbar_arrive(full0 + 8 * sidx);
         }
       }
@@ -1085,7 +1105,7 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
         const double dl = (double)(i - lane) - C.px[lane], dr = dl + 31.0;
         const double dx = dl > 0.0 ? dl : (dr < 0.0 ? -dr : 0.0);
         const double dy = (double)j - C.py[lane];
-        const double reach = C.pr[lane] + 0.5 * m.zeta + 1e-3;
+        const double reach = 0.5 * C.pd[lane] + 0.5 * m.zeta + 1e-3;
         nr = dx * dx + dy * dy < reach * reach;
       }
       near = __ballot_sync(0xffffffffu, nr);
@@ -1100,9 +1120,9 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
         const double dj = (double)j - C.py[c];
         T phi;
         if (F64)
-          phi = (T)phi_double(di, dj, C.pr[c], m.zeta, m.pi);
+          phi = (T)phi_double(di, dj, 0.5 * C.pd[c], m.zeta, m.pi);
         else
-          phi = (T)phi_float((float)di, (float)dj, (float)C.pr[c], m.zeta_f, m.pi_f);
+          phi = (T)phi_float((float)di, (float)dj, (float)(0.5 * C.pd[c]), m.zeta_f, m.pi_f);
         if (phi > (T)0) {
           hit = true;
           const T uxp = (T)C.pu[c] - (T)C.pw[c] * (T)dj;
@@ -1204,6 +1224,14 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? LBM_STEP_MINB_F64 :
       rec[3 * P + nd] = (T)no.yield;
     }
   }
+}
+
+// FP32: two CTAs per SM; FP64: one (with 17 warps, one SM sub-partition
+// holds 5 of them, which caps FP64 at 96 registers per thread).
+template <class T>
+__global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F32)
+    k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm) {
+  step_body<T>(a, tm);
 }
 
 template <class T>
