@@ -397,6 +397,24 @@ __device__ __forceinline__ void pull_interior(const T* __restrict__ src, const G
 }
 
 // ---------------------------------------------------------------------------
+// Warp sums of three values with 12 shuffles instead of 30: after the
+// exchange over lane bit 4 a lane keeps two of four partial sums (the fourth
+// is zero), after bit 3 one, then three plain levels.  Returns the total of
+// a in lanes 0-7, of b in lanes 8-15, of c in lanes 16-23.
+__device__ __forceinline__ double warp_sum3(double a, double b, double c, int lane) {
+  const bool hi = (lane & 16) != 0, mid = (lane & 8) != 0;
+  double k0 = hi ? c : a, k1 = hi ? 0.0 : b;
+  const double s0 = hi ? a : c, s1 = hi ? b : 0.0;
+  k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+  k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+  double k = mid ? k1 : k0;
+  k += __shfl_xor_sync(0xffffffffu, mid ? k0 : k1, 8);
+  k += __shfl_xor_sync(0xffffffffu, k, 4);
+  k += __shfl_xor_sync(0xffffffffu, k, 2);
+  k += __shfl_xor_sync(0xffffffffu, k, 1);
+  return k;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -714,6 +732,10 @@ struct Stage {
   static constexpr int BW = TW + 2 * H;                       // box width (544 bytes)
   static constexpr int PLANE = TR * BW;                       // elements per plane box
   static constexpr int BYTES = 9 * PLANE * (int)sizeof(T);
+  // offset of population k of a node from its column in the stage
+  __host__ __device__ static constexpr int off(int k) {
+    return plane_of(k) * PLANE + ((k == 1 || k == 5 || k == 8) ? -1 : (k == 3 || k == 6 || k == 7) ? 1 : 0);
+  }
 };
 
 #ifndef LBM_STEP_STAGES
@@ -834,13 +856,15 @@ __device__ __forceinline__ void cand_copy(const LatticeArgs& a, CandList c, int 
 #define LBM_STEP_MINB_F32 2
 #endif
 
-template <class T>
+// STRESS: the model needs the strain rate (Bingham viscosity or recorded
+// stress); the Newtonian instantiation carries none of that code.
+template <class T, bool STRESS>
 __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMap& tm) {
   constexpr bool F64 = sizeof(T) == 8;
   constexpr uint32_t WAIT = 1u << 20;
   using ST = Stage<T>;
   extern __shared__ __align__(128) unsigned char s_raw[];
-  const T* stage = reinterpret_cast<const T*>(s_raw);
+  T* const stage_w = reinterpret_cast<T*>(s_raw);
   const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(s_raw);
   const uint32_t full0 = s_base + NSTAGE * ST::BYTES;  // NSTAGE "full" barriers
   const uint32_t empty0 = full0 + 8 * NSTAGE;          // NSTAGE "empty" barriers
@@ -1043,19 +1067,13 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     const bool act = (i <= g.nx) && (j <= g.ny);
     const bool edge = (i == 0) || (i >= g.nx) || (j == 0) || (j >= g.ny);
     T f[9];
+    // this node's nine stage elements: planes in plane_of order, the row
+    // shift is in the box, the column shift -c_x is applied here.  Pull
+    // streaming is a bijection, so no other node reads these elements.
+    T* const q = stage_w + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
     if (!edge) {
-      const T* q = stage + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
-      // planes in plane_of order; the row shift is in the box, the column
-      // shift -c_x is applied here
-      f[0] = q[0];
-      f[1] = q[plane_of(1) * ST::PLANE - 1];
-      f[2] = q[plane_of(2) * ST::PLANE];
-      f[3] = q[plane_of(3) * ST::PLANE + 1];
-      f[4] = q[plane_of(4) * ST::PLANE];
-      f[5] = q[plane_of(5) * ST::PLANE - 1];
-      f[6] = q[plane_of(6) * ST::PLANE + 1];
-      f[7] = q[plane_of(7) * ST::PLANE + 1];
-      f[8] = q[plane_of(8) * ST::PLANE - 1];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
     } else if (act) {
       pull_bc<T>(src, g, m.bc, i, j, f);
     } else {
@@ -1087,6 +1105,12 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       rho = (T)1;
       drho = (T)0;
       ux = uy = (T)0;
+    }
+    // FP64 reads f back from the stage after the particle loop instead of
+    // holding 18 registers across it; edge nodes park theirs there first
+    if (F64 && edge && act) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) q[ST::off(k)] = f[k];
     }
 
     // ---- SPM body force (the highest-index particle with PHI>0 sets G,
@@ -1139,21 +1163,23 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
         }
       }
       if (__any_sync(0xffffffffu, hit)) {
-        fx = warp_sum(fx);
-        fy = warp_sum(fy);
-        tz = warp_sum(tz);
+        // warp totals of (Fx, Fy, Tz) in lanes 0, 8, 16
+        const double tot = warp_sum3(fx, fy, tz, lane);
         if (!waited) {  // the particle kernel has zeroed the accumulators
           asm volatile("griddepcontrol.wait;" ::: "memory");
           waited = true;
         }
-        if (lane == 0) {
-          unsigned long long* acc = a.facc + C.idx[c];
+        const int q = lane >> 3;
+        if ((lane & 7) == 0 && q < 3) {
           const long long st = a.npad;
-          facc_add(acc, acc + st, fx);
-          facc_add(acc + 2 * st, acc + 3 * st, fy);
-          facc_add(acc + 4 * st, acc + 5 * st, tz);
+          unsigned long long* acc = a.facc + C.idx[c] + 2 * q * st;
+          facc_add(acc, acc + st, tot);
         }
       }
+    }
+    if (F64 && act) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
     }
     // the stage and its candidates are consumed
     __syncwarp();
@@ -1172,16 +1198,17 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // ---- velocity correction (C1:1138-1152) and collision of the next step
     const T uxc = ux + (T)0.5 * (gx + (T)0.0);
     const T uyc = uy + (T)0.5 * (gy + (T)0.0);
-    const bool want_stress = m.bingham || m.record_stress;
+    const bool want_stress = STRESS;
+    const bool bingham = STRESS && m.bingham;
     NodeOut no;
     no.omega = m.omega;
     no.yield = 0;
     no.t11 = no.t22 = no.t12 = 0.0;
     T omn = (T)m.omega;
-    if (m.bingham) omn = static_cast<const T*>(a.om_src)[nd];
+    if (bingham) omn = static_cast<const T*>(a.om_src)[nd];
     if (F64) {
       double S[9];
-      if (m.bingham) {
+      if (bingham) {
         rates_double(m, (double)omn, S);
       } else {
 #pragma unroll
@@ -1198,7 +1225,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       Rates32 r;
       r.s1 = m.s_e_f;
       r.s2 = m.s_eps_f;
-      if (m.bingham) {
+      if (bingham) {
         const float w = (float)omn;
         r.sw = w;
         r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : m.sq_uni_f;
@@ -1214,8 +1241,8 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) dst[plane_of(k) * P + nd] = f[k];
-    if (m.bingham) static_cast<T*>(a.om_dst)[nd] = (T)no.omega;
-    if (m.record_stress) {
+    if (bingham) static_cast<T*>(a.om_dst)[nd] = (T)no.omega;
+    if (STRESS && m.record_stress) {
       const int slot = (kpar + 1) & 1;
       T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * P;
       rec[nd] = (T)no.t11;
@@ -1228,37 +1255,39 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
 
 // FP32: two CTAs per SM; FP64: one (with 17 warps, one SM sub-partition
 // holds 5 of them, which caps FP64 at 96 registers per thread).
-template <class T>
+template <class T, bool STRESS>
 __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F32)
     k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm) {
-  step_body<T>(a, tm);
+  step_body<T, STRESS>(a, tm);
 }
 
 template <class T>
 cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s) {
   using ST = Stage<T>;
   constexpr int SMEM = step_smem<T>();
-  static int grid_of[64] = {};
+  const int sx = (a.m.bingham || a.m.record_stress) ? 1 : 0;
+  void (*const kern)(const LatticeArgs, const CUtensorMap) = sx ? k_step<T, true> : k_step<T, false>;
+  static int grid_of[2][64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
-  if (grid_of[dev] == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+  if (grid_of[sx][dev] == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_step<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<T>, STEP_TPB, SMEM);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, STEP_TPB, SMEM);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     // one SM stays free for the particle kernel that runs beside the
     // particle-free tiles (it fills an SM's register file on its own)
-    grid_of[dev] = (per_sm > 0 ? per_sm : 1) * (sms > 1 ? sms - 1 : 1);
+    grid_of[sx][dev] = (per_sm > 0 ? per_sm : 1) * (sms > 1 ? sms - 1 : 1);
   }
   const int ntiles = ((a.g.nx + 1 + ST::TW - 1) / ST::TW) * ((a.g.ny + 1 + ST::TR - 1) / ST::TR);
-  const int grid = ntiles < grid_of[dev] ? ntiles : grid_of[dev];
+  const int grid = ntiles < grid_of[sx][dev] ? ntiles : grid_of[sx][dev];
   // Programmatic dependent launch: the kernel may start as soon as the
   // particle kernel before it on the stream allows (griddepcontrol.
   // launch_dependents); it waits for that kernel (griddepcontrol.wait) before
@@ -1273,7 +1302,7 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_step<T>, a, *tm);
+  return cudaLaunchKernelEx(&cfg, kern, a, *tm);
 }
 
 template <class T>
