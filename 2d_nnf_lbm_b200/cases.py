@@ -12,16 +12,19 @@ from __future__ import annotations
 import numpy as np
 
 from .lbm2d import (
+    LBM_BC_EQUILIBRIUM,
     LBM_BC_HALFWAY_BB,
     LBM_BINGHAM,
     LBM_CONTACT_DPP,
     LBM_CONTACT_STALE_DPW,
     LBM_FP64,
+    LBM_MOTION_OSCILLATE,
     LBM_NEWTONIAN,
     LBM_PIN,
     LBM_RATES_FIXED_Q,
     LBM_RATES_Q_OF_OMEGA,
     LBM_WALL_MIRROR,
+    LBM_WALL_NONE,
     LBM_WALL_OFFSET,
     LbmParams,
     glowinski_cij,
@@ -119,6 +122,31 @@ def shipped_c6(nx: int = 80, ny: int = 300) -> tuple[LbmParams, np.ndarray]:
     p.e_w = p.e_p
     p.c_ij = glowinski_cij(rho_s, rho_f, a_g, p.pi, l_c)
     disk = pin_array([[0.5 * float(nx), float(ny) - 7.0 * l_c]], l_c, rho_s)
+    return p, disk
+
+
+def shipped_c4(nx: int = 1500, ny: int = 1000, l_c: float = 50.0, re_t: float = 100.0,
+               t_c: float | None = None) -> tuple[LbmParams, np.ndarray]:
+    """4_Oscillating_Particle (C4:2-93, C4:197-214): a cylinder D = L_C,
+    rho_p = RHO_S = 1, at the centre, driven at u = -U_C cos(2 PI KK/T_C)
+    (C4:226), equilibrium boundary on every edge (C4:1219-1275), rates
+    1.6 / 1.8 / q(omega) (C4:1018), no gravity.  U_C = RE_T*NU/L_C (C4:30),
+    T_C = 5*L_C/U_C (C4:32) unless given; returns params and the disk."""
+    p = LbmParams(nx=nx, ny=ny)
+    nu = r4(0.025)
+    u_c = re_t * nu / l_c
+    if t_c is None:
+        t_c = 5.0 * l_c / u_c
+    p.nu = nu
+    p.bc = LBM_BC_EQUILIBRIUM
+    p.rate_set = LBM_RATES_Q_OF_OMEGA
+    p.s_e, p.s_eps = r4(1.6), r4(1.8)
+    p.gravity = 0.0
+    p.wall_model = LBM_WALL_NONE
+    p.motion = LBM_MOTION_OSCILLATE
+    p.osc_u, p.osc_period = u_c, t_c
+    p.zeta = 1.0
+    disk = pin_array([[0.5 * float(nx), 0.5 * float(ny)]], l_c, 1.0, uvw=[[-u_c, 0.0, 0.0]])
     return p, disk
 
 

@@ -35,6 +35,8 @@ struct lbm_sim {
   void* f[2] = {nullptr, nullptr};
   void* om[2] = {nullptr, nullptr};
   void* rec = nullptr;
+  void* ring = nullptr;  // equilibrium boundary: T[2][3][ring_n]
+  int ring_n = 0;
   int cur = 0;
   bool prev_post_bc = false;
   int64_t kk = 0;
@@ -177,6 +179,8 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.mass_acc = h->series ? h->mass_acc : nullptr;
   a.status = h->d_status;
   a.rec = h->rec;
+  a.ring = h->ring;
+  a.ring_n = h->ring_n;
   return a;
 }
 
@@ -229,6 +233,10 @@ ParticleArgs particle_args(lbm_sim* h) {
   a.nx = h->p.nx;
   a.ny = h->p.ny;
   a.zeta = h->p.zeta;
+  a.motion = h->p.motion;
+  a.osc_u = h->p.osc_u;
+  a.osc_period = h->p.osc_period;
+  a.pi = h->p.pi;
   return a;
 }
 
@@ -494,6 +502,7 @@ void destroy_buffers(lbm_sim* h) {
     dfree(h->om[b]);
   }
   dfree(h->rec);
+  dfree(h->ring);
   dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
   dfree(h->tile_count); dfree(h->tile_list); dfree(h->tile_cur); dfree(h->pair_rebuild);
   dfree(h->tile_order); dfree(h->n_unlisted); dfree(h->work_ctr);
@@ -570,6 +579,9 @@ int lbm_compute_error(lbm_sim* h, double* er) {
   return refreshed_status(h);
 }
 
+static_assert(lbm::BC_EQUILIBRIUM == LBM_BC_EQUILIBRIUM, "kernel switch values");
+static_assert(lbm::MOTION_OSCILLATE == LBM_MOTION_OSCILLATE, "kernel switch values");
+
 int lbm_params_init(lbm_params* p) {
   if (!p) return LBM_E_INVALID;
   std::memset(p, 0, sizeof(*p));
@@ -630,7 +642,11 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   const lbm_params& p = *pin;
   if (p.nx < 2 || p.ny < 2 || (long long)(p.nx + 1) * (p.ny + 1) > (1LL << 31)) return LBM_E_INVALID;
   if (p.precision != LBM_FP64 && p.precision != LBM_FP32_SHIFTED) return LBM_E_INVALID;
-  if (p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB) return LBM_E_INVALID;
+  if (p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB && p.bc != LBM_BC_EQUILIBRIUM)
+    return LBM_E_INVALID;
+  if (p.motion != LBM_MOTION_FREE && p.motion != LBM_MOTION_OSCILLATE) return LBM_E_INVALID;
+  if (p.motion == LBM_MOTION_OSCILLATE && (!std::isfinite(p.osc_u) || !(p.osc_period > 0.0)))
+    return LBM_E_INVALID;
   if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM) return LBM_E_INVALID;
   if (p.wall_model < 0 || p.wall_model > 2 || p.contact_test < 0 || p.contact_test > 1)
     return LBM_E_INVALID;
@@ -696,6 +712,11 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   m.s_eps_f = (float)p.s_eps;
   m.sq_uni_f = (float)oq;
   m.omega_f = (float)omega;
+  for (int k = 0; k < 3; ++k) m.w_init_f[k] = (float)p.w_init[k];
+  for (int k = 0; k < 9; ++k) {  // rho0*(W_k*B_k(u=0) - w_k), B(0) = 2 (k<5) or 1
+    const double W = p.w_init[k == 0 ? 0 : (k < 5 ? 1 : 2)];
+    m.eq_c_f[k] = (float)(p.rho0 * (W * (k < 5 ? 2.0 : 1.0) - w[k]));
+  }
 
   int rc = LBM_OK;
   auto fail = [&](int code) {
@@ -720,6 +741,12 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if (m.record_stress &&
       cudaMalloc(&h->rec, (size_t)2 * 4 * h->g.plane * h->esz) != cudaSuccess)
     return fail(LBM_E_NOMEM);
+  if (p.bc == LBM_BC_EQUILIBRIUM) {
+    h->ring_n = 2 * (p.nx + 1) + 2 * (p.ny + 1);
+    const size_t rb = (size_t)2 * 3 * h->ring_n * h->esz;
+    if (cudaMalloc(&h->ring, rb) != cudaSuccess) return fail(LBM_E_NOMEM);
+    cudaMemsetAsync(h->ring, 0, rb, h->stream);
+  }
   if ((rc = make_tensor_maps(h))) return fail(rc);
   const int ntiles = h->g.ltx * h->g.lty;
   if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);

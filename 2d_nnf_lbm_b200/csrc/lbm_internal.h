@@ -18,6 +18,11 @@
 
 namespace lbm {
 
+// Switch values of lbm_params the kernels test (equal to the lbm2d.h enums;
+// lbm_api.cu asserts it).
+constexpr int BC_EQUILIBRIUM = 2;     // LBM_BC_EQUILIBRIUM
+constexpr int MOTION_OSCILLATE = 1;   // LBM_MOTION_OSCILLATE
+
 // Scalar lattice kernels: one node per thread, blocks of TX x TY nodes.
 constexpr int TX = 32;
 constexpr int TY = 8;
@@ -94,6 +99,9 @@ struct Model {
   float rho0_f, nu_f, d_mrt_f, pi_f, zeta_f, tau_y_f, m_pap_f, gamma_min_f;
   float s_e_f, s_eps_f, sq_uni_f, omega_f;
   float shift_f[9];  // rho0*w_k*(36*d_mrt - 1)
+  // equilibrium boundary in FP32: COMPUTEFEQNEW weights and, per k,
+  // rho0*(W_k*B_k(u=0) - w_k) of the shifted form
+  float w_init_f[3], eq_c_f[9];
 };
 
 struct ParticleArgs {
@@ -109,6 +117,8 @@ struct ParticleArgs {
   int* work_ctr;             // [2]: step-kernel tile queue of step k at [k&1]
   int tile_cap;
   int ntiles, nbx;
+  int motion;                // LBM_MOTION_*
+  double osc_u, osc_period, pi;
   int* nbr;                  // [MAX_NEIGH][npad]
   int* nbr_count;            // [npad]
   double* nbr_xy;            // [2][npad] centres at the last pair-list build
@@ -149,6 +159,10 @@ struct LatticeArgs {
   int* work_ctr;         // [2]: tile queue of step k at [k&1], zero at the start
   int tile_cap;
   int ntiles;
+  // equilibrium boundary: density (FP32: rho - rho0) and corrected velocity
+  // of the nodes next to the edges, T[2 parities][3][ring_n]
+  void* ring;
+  int ring_n;
   unsigned long long* facc;  // [6][npad]
   long long step;        // lattice step of this launch
   int rec_slot;          // history slot of this step (-1: none)

@@ -56,6 +56,74 @@ __device__ __forceinline__ void feq_double(const Model& m, double ux, double uy,
   feq[8] = W2 * rho * (1. + 3. * (ux - uy) - 9. * ux * uy + 3. * U2);
 }
 
+// ---------------------------------------------------------------------------
+// Equilibrium boundary (C4:1219-1275): each edge node takes COMPUTEFEQNEW of
+// the density and corrected velocity its inward neighbour had in the
+// previous step (corners: the diagonal neighbour).  Those values of the
+// nodes next to the edges are kept in a ring, one per step parity:
+// [par][rho | ux | uy][slot], slots: row j = 1 at i, row j = NY-1 at
+// NX+1+i, column i = 1 at 2(NX+1)+j, column i = NX-1 at 2(NX+1)+NY+1+j.
+__device__ __forceinline__ int ring_edge_slot(const Geometry& g, int i, int j) {
+  const int ii = i < 1 ? 1 : (i > g.nx - 1 ? g.nx - 1 : i);
+  if (j == 0) return ii;
+  if (j == g.ny) return g.nx + 1 + ii;
+  if (i == 0) return 2 * (g.nx + 1) + j;
+  return 2 * (g.nx + 1) + g.ny + 1 + j;  // i == NX
+}
+
+template <class T>
+__device__ __forceinline__ void ring_store(const LatticeArgs& a, int i, int j, int par, T r,
+                                           T ux, T uy) {
+  const Geometry& g = a.g;
+  if (i < 1 || i > g.nx - 1 || j < 1 || j > g.ny - 1) return;
+  T* q = static_cast<T*>(a.ring) + (long long)par * 3 * a.ring_n;
+  const int n = a.ring_n;
+  if (j == 1) { q[i] = r; q[n + i] = ux; q[2 * n + i] = uy; }
+  if (j == g.ny - 1) { const int s = g.nx + 1 + i; q[s] = r; q[n + s] = ux; q[2 * n + s] = uy; }
+  if (i == 1) { const int s = 2 * (g.nx + 1) + j; q[s] = r; q[n + s] = ux; q[2 * n + s] = uy; }
+  if (i == g.nx - 1) {
+    const int s = 2 * (g.nx + 1) + g.ny + 1 + j;
+    q[s] = r; q[n + s] = ux; q[2 * n + s] = uy;
+  }
+}
+
+// f of edge node (i, j) from the ring of parity par.  FP64: the reference's
+// arithmetic.  FP32 (shifted populations, the ring holding rho - rho0):
+// h_k = W_k (drho B_k + rho0 (B_k - B_k(0))) + rho0 (W_k B_k(0) - w_k), with
+// B_k the bracket of COMPUTEFEQNEW, so no O(1) terms cancel.
+template <class T>
+__device__ __forceinline__ void edge_equilibrium(const LatticeArgs& a, int i, int j, int par,
+                                                 T* f) {
+  const int s = ring_edge_slot(a.g, i, j), n = a.ring_n;
+  const T* q = static_cast<const T*>(a.ring) + (long long)par * 3 * n;
+  const T r = q[s], ux = q[n + s], uy = q[2 * n + s];
+  if (sizeof(T) == 8) {
+    double fe[9];
+    feq_double(a.m, (double)ux, (double)uy, (double)r, fe);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (T)fe[k];
+    return;
+  }
+  const float x = (float)ux, y = (float)uy, dr = (float)r, r0 = a.m.rho0_f;
+  const float U2 = x * x + y * y;
+  float d[9];  // B_k - B_k(0)
+  d[0] = -3.f * U2;
+  d[1] = 6.f * x + 9.f * x * x - 3.f * U2;
+  d[2] = 6.f * y + 9.f * y * y - 3.f * U2;
+  d[3] = -6.f * x + 9.f * x * x - 3.f * U2;
+  d[4] = -6.f * y + 9.f * y * y - 3.f * U2;
+  d[5] = 3.f * (x + y) + 9.f * x * y + 3.f * U2;
+  d[6] = -3.f * (x - y) - 9.f * x * y + 3.f * U2;
+  d[7] = -3.f * (x + y) + 9.f * x * y + 3.f * U2;
+  d[8] = 3.f * (x - y) - 9.f * x * y + 3.f * U2;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const float W = a.m.w_init_f[k == 0 ? 0 : (k < 5 ? 1 : 2)];
+    const float B = (k == 0 || k < 5 ? 2.f : 1.f) + d[k];
+    f[k] = (T)(W * (dr * B + r0 * d[k]) + a.m.eq_c_f[k]);
+  }
+}
+
 // ComputeRelaxation_MRT (C1:1029-1048 fixed q; C6:1002-1021 q of omega).
 __device__ __forceinline__ void rates_double(const Model& m, double omega, double* S) {
   const double oq = m.q_of_omega ? 8. * (2. - omega) / (8. - omega) : m.s_q;
@@ -522,8 +590,11 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
       const bool interior = blockIdx.x > 0 && blockIdx.y > 0 &&
                             (int)(blockIdx.x + 1) * TX <= g.nx &&
                             (int)(blockIdx.y + 1) * TY <= g.ny;
+      const bool on_edge = i == 0 || i == g.nx || j == 0 || j == g.ny;
       if (interior)
         pull_interior<T>(src, g, n, f);
+      else if (m.bc == BC_EQUILIBRIUM && on_edge)
+        edge_equilibrium<T>(a, i, j, (int)((a.step - 1) & 1), f);
       else
         pull_bc<T>(src, g, m.bc, i, j, f);
     }
@@ -619,6 +690,8 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
   // ---- velocity correction (C1:1138-1152) --------------------------------
   const T uxc = ux + (T)0.5 * (gx + (T)0.0);
   const T uyc = uy + (T)0.5 * (gy + (T)0.0);
+  if ((MODE == MODE_INIT || MODE == MODE_RESTART) && m.bc == BC_EQUILIBRIUM && act)
+    ring_store<T>(a, i, j, (int)(a.step & 1), F64 ? rho : drho, uxc, uyc);
 
   if (MODE == MODE_OUTPUT) {
     if (act) {
@@ -1075,7 +1148,10 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
 #pragma unroll
       for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
     } else if (act) {
-      pull_bc<T>(src, g, m.bc, i, j, f);
+      if (m.bc == BC_EQUILIBRIUM)
+        edge_equilibrium<T>(a, i, j, (int)((a.step - 1) & 1), f);
+      else
+        pull_bc<T>(src, g, m.bc, i, j, f);
     } else {
 #pragma unroll
       for (int k = 0; k < 9; ++k) f[k] = (T)0;
@@ -1198,6 +1274,8 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // ---- velocity correction (C1:1138-1152) and collision of the next step
     const T uxc = ux + (T)0.5 * (gx + (T)0.0);
     const T uyc = uy + (T)0.5 * (gy + (T)0.0);
+    if (m.bc == BC_EQUILIBRIUM)
+      ring_store<T>(a, i, j, (int)(a.step & 1), F64 ? rho : drho, uxc, uyc);
     const bool want_stress = STRESS;
     const bool bingham = STRESS && m.bingham;
     NodeOut no;

@@ -379,15 +379,27 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
     P[P_FCX] = fcx;
     P[P_FCY] = fcy;
 
-    // Newton-Euler with internal-mass correction (C1:250-258, C6:312)
+    // Newton-Euler with internal-mass correction (C1:250-258, C6:312), or
+    // the prescribed oscillation (C4:222-228) with F_H_IN of this step's
+    // velocity change (C4:270-272)
     const double RHO0 = a.rho0;
     const double rr = RHO0 / rhop;
-    const double fh0 = rr * M * (u0 - uo0);
-    const double fh1 = rr * M * (u1 - uo1);
-    const double fh2 = rr * I * (u2 - uo2);
-    const double v0 = u0 + frx / M + fh0 / M + fcx / M;
-    const double v1 = u1 + fry / M + fh1 / M + (1.0 - RHO0 / rhop) * a.gravity + fcy / M;
-    const double v2 = u2 + frt / I + fh2 / I;
+    double fh0, fh1, fh2, v0, v1, v2;
+    if (a.motion == MOTION_OSCILLATE) {
+      v0 = -(a.osc_u * cos(((2.0 * a.pi) * (double)s_kk) / a.osc_period));
+      v1 = 0.0;
+      v2 = 0.0;
+      fh0 = rr * M * (v0 - u0);
+      fh1 = rr * M * (v1 - u1);
+      fh2 = rr * I * (v2 - u2);
+    } else {
+      fh0 = rr * M * (u0 - uo0);
+      fh1 = rr * M * (u1 - uo1);
+      fh2 = rr * I * (u2 - uo2);
+      v0 = u0 + frx / M + fh0 / M + fcx / M;
+      v1 = u1 + fry / M + fh1 / M + (1.0 - RHO0 / rhop) * a.gravity + fcy / M;
+      v2 = u2 + frt / I + fh2 / I;
+    }
     const double nx_ = px + 0.5 * (v0 + u0);
     const double ny_ = py + 0.5 * (v1 + u1);
     P[P_FHX] = fh0;

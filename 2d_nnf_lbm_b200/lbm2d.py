@@ -35,7 +35,8 @@ ERRORS = {
     -10: "LBM_E_ABI",
 }
 LBM_FP64, LBM_FP32_SHIFTED = 0, 1
-LBM_BC_ZOUHE, LBM_BC_HALFWAY_BB = 0, 1
+LBM_BC_ZOUHE, LBM_BC_HALFWAY_BB, LBM_BC_EQUILIBRIUM = 0, 1, 2
+LBM_MOTION_FREE, LBM_MOTION_OSCILLATE = 0, 1
 LBM_NEWTONIAN, LBM_BINGHAM = 0, 1
 LBM_RATES_FIXED_Q, LBM_RATES_Q_OF_OMEGA = 0, 1
 LBM_WALL_MIRROR, LBM_WALL_OFFSET, LBM_WALL_NONE = 0, 1, 2
@@ -82,7 +83,7 @@ class LbmParams(ctypes.Structure):
         ("series_capacity", ctypes.c_int32),
         ("record_stress", ctypes.c_int32),
         ("device", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("motion", ctypes.c_int32),
         ("nu", ctypes.c_double),
         ("rho0", ctypes.c_double),
         ("s_e", ctypes.c_double),
@@ -105,6 +106,8 @@ class LbmParams(ctypes.Structure):
         ("c_ij", ctypes.c_double),
         ("wall_mirror_top", ctypes.c_double),
         ("wall_mirror_left", ctypes.c_double),
+        ("osc_u", ctypes.c_double),
+        ("osc_period", ctypes.c_double),
     ]
 
     def __init__(self, **kw):

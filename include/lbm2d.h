@@ -51,7 +51,16 @@ enum { LBM_FP64 = 0,            /* plain populations in FP64 (drop-in)        */
        LBM_FP32_SHIFTED = 1 };  /* FP32 storage of f - w_i*rho0, FP32 math    */
 
 enum { LBM_BC_ZOUHE = 0,        /* C1:1250-1258, C1:1341-1363 + corners        */
-       LBM_BC_HALFWAY_BB = 1 }; /* C6:1206-1219, C6:1285-1294 + corners        */
+       LBM_BC_HALFWAY_BB = 1,   /* C6:1206-1219, C6:1285-1294 + corners        */
+       LBM_BC_EQUILIBRIUM = 2   /* C4:1219-1275: every edge node takes the
+                                   equilibrium of its inward neighbour's density
+                                   and velocity of the previous step           */ };
+
+enum { LBM_MOTION_FREE = 0,      /* Newton-Euler (C1:247-259)                   */
+       LBM_MOTION_OSCILLATE = 1  /* prescribed u = -osc_u*cos(2*PI*kk/osc_period),
+                                    v = w = 0 (C4:222-228); FORCE is still
+                                    computed, F_H_IN from this step's change
+                                    (C4:270-272)                               */ };
 
 enum { LBM_NEWTONIAN = 0,
        LBM_BINGHAM = 1 };       /* Papanastasiou-regularised, C6:913-958       */
@@ -88,7 +97,7 @@ typedef struct lbm_params {
     int32_t series_capacity;  /* records buffered on the device                */
     int32_t record_stress;    /* 1: keep stress / yield flag / omega fields    */
     int32_t device;           /* CUDA device ordinal                           */
-    int32_t reserved0;
+    int32_t motion;           /* LBM_MOTION_*                                  */
 
     double nu;                /* NU (plastic viscosity Mu_0 for Bingham)       */
     double rho0;              /* RHO0, C1:57                                   */
@@ -108,6 +117,8 @@ typedef struct lbm_params {
     double c_ij;              /* CIJ = -(RHO_S-RHO_F)*A_G*PI*R^2 (C1:701)      */
     double wall_mirror_top;   /* 2*WALL%EDGE(3) (C1:741)                       */
     double wall_mirror_left;  /* 2*WALL%EDGE(4) (C1:743)                       */
+    double osc_u;             /* U_C of LBM_MOTION_OSCILLATE (C4:30)           */
+    double osc_period;        /* T_C of LBM_MOTION_OSCILLATE (C4:32)           */
 } lbm_params;
 
 /* Particle input record (lbm_set_particles): LBM_PIN doubles per disk. */

@@ -377,6 +377,30 @@ static void bc_halfway(oracle* o) {
 #undef F_
 #undef FP_
 
+/* ---- BOUNDARYCONDITION of the oscillating-cylinder case, C4:1219-1275:
+ * every edge node takes COMPUTEFEQNEW of the density and velocity that its
+ * inward neighbour holds at this point of the step (those of the previous
+ * step, after VelocityCorrector); corners take the diagonal neighbour. */
+static void bc_equilibrium(oracle* o) {
+    const int NX = o->nx, NY = o->ny;
+    for (int i = 1; i <= NX - 1; ++i) {                          /* C4:1219-1223 */
+        size_t a = IDX(o, i, 1), b = IDX(o, i, NY - 1);
+        compute_feq(o, o->UX[a], o->UY[a], o->RHO[a], &FK(o, o->F, 0, i, 0));
+        compute_feq(o, o->UX[b], o->UY[b], o->RHO[b], &FK(o, o->F, 0, i, NY));
+    }
+    for (int j = 1; j <= NY - 1; ++j) {                          /* C4:1263-1266 */
+        size_t a = IDX(o, 1, j), b = IDX(o, NX - 1, j);
+        compute_feq(o, o->UX[a], o->UY[a], o->RHO[a], &FK(o, o->F, 0, 0, j));
+        compute_feq(o, o->UX[b], o->UY[b], o->RHO[b], &FK(o, o->F, 0, NX, j));
+    }
+    const int ci[4][4] = {{0, 0, 1, 1}, {0, NY, 1, NY - 1}, {NX, NY, NX - 1, NY - 1},
+                          {NX, 0, NX - 1, 1}};                    /* C4:1268-1273 */
+    for (int c = 0; c < 4; ++c) {
+        size_t a = IDX(o, ci[c][2], ci[c][3]);
+        compute_feq(o, o->UX[a], o->UY[a], o->RHO[a], &FK(o, o->F, 0, ci[c][0], ci[c][1]));
+    }
+}
+
 /* ---- MACROSCOPICVARIABLES, C1:1421-1439 ------------------------------- */
 static void macroscopic(oracle* o) {
     for (int j = 0; j <= o->ny; ++j)
@@ -530,6 +554,20 @@ static void particle_update(oracle* o) {
         double* V = d->vel;
         double* VO = d->vp_old;
         double* FH = d->fh_in;
+        if (o->p.motion == LBM_MOTION_OSCILLATE) {
+            /* prescribed oscillation, C4:222-228; F_H_IN of this step's
+             * change, C4:270-272 */
+            VO[0] = V[0]; VO[1] = V[1]; VO[2] = V[2];
+            V[0] = -(o->p.osc_u * cos(((2.0 * o->p.pi) * (double)o->kk) / o->p.osc_period));
+            V[1] = 0.0;
+            V[2] = 0.0;
+            d->center[0] = d->center[0] + 0.5 * (V[0] + VO[0]);
+            d->center[1] = d->center[1] + 0.5 * (V[1] + VO[1]);
+            FH[0] = (RHO0 / d->rho_p) * d->m_p * (V[0] - VO[0]);
+            FH[1] = (RHO0 / d->rho_p) * d->m_p * (V[1] - VO[1]);
+            FH[2] = (RHO0 / d->rho_p) * d->i_p * (V[2] - VO[2]);
+            continue;
+        }
         FH[0] = (RHO0 / d->rho_p) * d->m_p * (V[0] - VO[0]);
         FH[1] = (RHO0 / d->rho_p) * d->m_p * (V[1] - VO[1]);
         FH[2] = (RHO0 / d->rho_p) * d->i_p * (V[2] - VO[2]);
@@ -588,7 +626,9 @@ static void one_step(oracle* o) {
     collision_mrt(o);
     memcpy(o->FPOST, o->F, Q * o->nn * sizeof(double));
     streaming(o);
-    if (o->p.bc == LBM_BC_ZOUHE) bc_zouhe(o); else bc_halfway(o);
+    if (o->p.bc == LBM_BC_ZOUHE) bc_zouhe(o);
+    else if (o->p.bc == LBM_BC_EQUILIBRIUM) bc_equilibrium(o);
+    else bc_halfway(o);
     macroscopic(o);
     force_field_spm(o);
     force_hydro(o);

@@ -21,6 +21,10 @@ named; only PARAMETERs and the particle input file are replaced):
              chain, rate set q(omega), angle integration
   c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
              the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
+  c4_oscillate  4_Oscillating_Particle (C4), NX=40 NY=30, L_C=10 (the disk
+             D=10 at the centre), RE_T=10 (U_C=0.025), T_C=40 (the loop runs
+             INT(6*T_C)=240 steps): prescribed u=-U_C*cos(2*PI*KK/T_C),
+             equilibrium boundary on every edge, rate set 1.6/1.8/q(omega)
   c3_multi   3_MultiParticle_Sedimentation (C3), NX=48 NY=72, N_PARTICLE=3
              (D = L_C = 16), 20 steps: pair repulsion including the stale
              D_PW contact test.  The STOP at C3:202, which ends the shipped
@@ -61,6 +65,10 @@ CASES = {
     "c6_bingham": dict(file="6_FreeFall_YieldStress/D2Q9_BinghamSediment_Validated_20191127.f90",
                        overrides={"NX": "24", "NY": "60", "TIME_MAX": "30"},
                        particles=None, steps=30),
+    "c4_oscillate": dict(file="4_Oscillating_Particle/D2Q9_V7_OscillatingCylinder_Validated.f90",
+                         overrides={"NX": "40", "NY": "30", "L_C": "10.0", "RE_T": "10.0",
+                                    "T_C": "40.0"},
+                         particles=None, steps=240),
     "c3_multi": dict(file="3_MultiParticle_Sedimentation/D2Q9_RTParticle_20191003.f90",
                      overrides={"NX": "48", "NY": "72", "TIME_MAX": "20", "N_PARTICLE": "3"},
                      particles="\t\n14\t50\n30.6\t50\n24\t22\n", steps=20, skip_lines=[202]),
@@ -80,9 +88,10 @@ def run_case(ref_root, name, spec):
     for k in ("F", "UX", "UY", "RHO", "G", "OMEGA_BN", "DOMAIN_IMAGE"):
         if k in frame:
             out[k] = np.asarray(frame[k])
-    for k in ("VP_OLD", "F_H_IN"):  # (1:3, 1:N) per-particle work arrays
+    for k in ("VP_OLD", "F_H_IN"):  # (1:3, 1:N) per-particle work arrays; (1:3) in C4
         if k in frame:
-            out[k] = np.asarray(frame[k])[:, :n_used]
+            v = np.asarray(frame[k])
+            out[k] = (v[:, None] if v.ndim == 1 else v)[:, :n_used]
     disks = frame["DISK"][:n_used]  # the main program may declare more than it uses
     for fld in PARTICLE_FIELDS:
         if hasattr(disks[0], fld):

@@ -262,3 +262,57 @@ def test_wall_column_pass(pkg, cases, nx, precision):
         a, b = sim.field(f), ref.field(f)
         sc = np.max(np.abs(b - (1.0 if f == "rho" else 0.0)))
         assert np.max(np.abs(a - b)) <= 1e-4 * max(sc, 1e-12), f
+
+
+# ---- case 4: prescribed oscillation, equilibrium boundary, 1.6/1.8 rates ---
+def _c4(cases):
+    return cases.shipped_c4(40, 30, 10.0, 10.0, 40.0)
+
+
+@pytest.mark.parametrize("precision,rtol", [(0, 1e-10), (1, 2e-4)])
+def test_c4_oscillating_cylinder_matches_reference_golden(pkg, cases, precision, rtol):
+    """The C4 fixture (the reference's own run, 240 steps): fields, the
+    populations after the equilibrium boundary, the disk, and the force
+    history the program writes to unit 11."""
+    g = _golden("c4_oscillate")
+    p, disk = _c4(cases)
+    p.precision = precision
+    p.series_every, p.series_particles, p.series_capacity = 1, 1, 512
+    sim = pkg.Simulation(p)
+    try:
+        sim.set_particles(disk)
+        sim.step(int(g["steps"]))
+        for f, ref in (("ux", g["UX"]), ("uy", g["UY"]), ("gx", g["G"][0]), ("gy", g["G"][1])):
+            close64(sim.field(f).T, ref, rtol, f"field {f}")
+        close64(sim.field("rho").T - 1.0, g["RHO"] - 1.0, rtol, "density deviation")
+        f, _, _ = sim.get_state()
+        n1x, n1y = p.nx + 1, p.ny + 1
+        close64(f.reshape(n1y, n1x, 9).transpose(2, 1, 0), g["F"], rtol, "F after BC")
+        gp = sim.particles()
+        close64(gp[:, 0:2], g["DISK_CENTER"], 1e-12, "centre")
+        close64(gp[:, 3:6], g["DISK_VELOCITY"], 1e-12, "prescribed velocity")
+        close64(gp[:, 6:8], g["DISK_FORCE"][:, 0:2], rtol, "force")
+        s = sim.series()
+        fx = np.append(s[1:, 2 + 6], gp[0, 6])
+        f_c = 0.5 * p.osc_u * p.osc_u * 10.0
+        hist = np.stack([s[:, 0] / p.osc_period, (fx + s[:, 2 + 9]) / f_c, fx / f_c], axis=1)
+        close64(hist, g["UNIT11"], rtol, "force history (unit 11)")
+    finally:
+        sim.close()
+
+
+def test_c4_checkpoint_roundtrip(pkg, cases):
+    """Restart under the equilibrium boundary: the neighbour values that the
+    boundary of the next step needs are rebuilt from the checkpoint."""
+    p, disk = _c4(cases)
+    a = pkg.Simulation(p)
+    a.set_particles(disk)
+    a.step(70)
+    f, om, parts = a.get_state()
+    a.step(30)
+    b = pkg.Simulation(p)
+    b.set_state(70, f, om, parts)
+    b.step(30)
+    assert np.array_equal(a.particles(), b.particles())
+    assert np.array_equal(a.field("ux"), b.field("ux"))
+    assert np.array_equal(a.field("rho"), b.field("rho"))

@@ -37,10 +37,13 @@ def _setup(cases, name):
                               float(np.float32(1.01)))
         # the reference's D_PW local starts at zero in the translated run
         return p, pin, {"stale_dpw_init": 0.0}
+    if name == "c4_oscillate":
+        p, disk = cases.shipped_c4(40, 30, 10.0, 10.0, 40.0)
+        return p, disk, {}
     raise KeyError(name)
 
 
-CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi"]
+CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c4_oscillate"]
 
 
 def _exact(a, b, what):
@@ -75,7 +78,8 @@ def test_oracle_reproduces_reference_bit_for_bit(cases, name):
         _exact(op[:, 0:2], g["DISK_CENTER"], "CENTER")
         _exact(op[:, 3:6], g["DISK_VELOCITY"], "VELOCITY")
         _exact(op[:, 6:9], g["DISK_FORCE"], "FORCE")
-        _exact(op[:, 9:11], g["DISK_F_COL"], "F_COL")
+        if name != "c4_oscillate":  # C4's Wan-Turek F_COL never reaches its outputs
+            _exact(op[:, 9:11], g["DISK_F_COL"], "F_COL")
         _exact(op[:, 14], g["DISK_M_P"], "M_P")
         _exact(op[:, 15], g["DISK_I_P"], "I_P")
         if "DISK_ANGLE" in g:
@@ -84,6 +88,15 @@ def test_oracle_reproduces_reference_bit_for_bit(cases, name):
         s = o.series()
         _exact(s[:, 0], g["UNIT8"][:, 0], "history step numbers")
         _exact(s[:, 1], g["UNIT8"][:, 1], "mean density per step (unit 8)")
+        if name == "c4_oscillate":
+            # unit 11 (C4:279): KK/T_C, (FORCE(1)+F_H_IN(1))/F_C, FORCE(1)/F_C
+            # after this step's lattice pass: FORCE of step k is the force
+            # the record of step k+1 starts with (the last one, the final state)
+            fx = np.append(s[1:, 2 + 6], op[0, 6])
+            u_c, t_c, l_c = p.osc_u, p.osc_period, 10.0
+            f_c = 0.5 * u_c * u_c * l_c
+            hist = np.stack([s[:, 0] / t_c, (fx + s[:, 2 + 9]) / f_c, fx / f_c], axis=1)
+            _exact(hist, g["UNIT11"], "force history (unit 11)")
     finally:
         o.close()
 
