@@ -171,6 +171,23 @@ def time_steps(pkg, torch, sim, k):
     return t0.elapsed_time(t1)
 
 
+def reduce_max(dist, torch, value, device):
+    """Max of a per-rank number over all ranks (a replica job takes as long
+    as its slowest rank); ``device`` is where the backend reduces: cuda:N for
+    NCCL, cpu for gloo."""
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world, nodes, steps, ms_max):
+    """Whole-job MLUPS of `world` replicas that each update `nodes` nodes
+    `steps` times, the slowest in `ms_max` milliseconds (weak scaling)."""
+    return world * nodes * steps / (ms_max * 1e-3) / 1e6
+
+
 def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False):
     p, pin = workload(pkg, precision, args)
     p.device = device
@@ -185,10 +202,7 @@ def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False)
         sampler.start()
     ms = time_steps(pkg, torch, sim, args.steps)
     clk = sampler.stop() if sampler else None
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(dist, torch, ms, f"cuda:{device}")
     status = sim.status()
     # Per-kernel durations: an identical pass of the same number of steps
     # with CUDA events recorded between the launches on the library's stream
@@ -331,15 +345,13 @@ def main():
     r64 = run_gpu_path(pkg, torch, args, 0, device, world, dist)
     e2e = run_e2e(pkg, torch, args, device)
     if dist is not None:
-        t = torch.tensor([1.0 / e2e["value"]], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["value"] = world / float(t.item())
+        e2e["value"] = world / reduce_max(dist, torch, 1.0 / e2e["value"], f"cuda:{device}")
 
     peak, peak_src = hbm_peak()
     ach32 = BYTES_PER_NODE[1] * r32["nodes"] / (r32["lattice_ms"] * 1e-3) / 1e9
     ach64 = BYTES_PER_NODE[0] * r64["nodes"] / (r64["lattice_ms"] * 1e-3) / 1e9
-    value = world * r32["nodes"] * args.steps / (r32["ms"] * 1e-3) / 1e6
-    value64 = world * r64["nodes"] * args.steps / (r64["ms"] * 1e-3) / 1e6
+    value = job_mlups(world, r32["nodes"], args.steps, r32["ms"])
+    value64 = job_mlups(world, r64["nodes"], args.steps, r64["ms"])
     line = {
         "metric": metric,
         "value": value,
