@@ -22,7 +22,10 @@
 // disk; VP_OLD, F_COL and F_H_IN start at zero as in a fresh reference
 // process, and the step counter starts at 0 (C1:235).
 //
-//   lbm_main --case c1|c6|c3 [--nx N] [--ny N] [--steps N] [--input FILE]
+//   C4 (4_Oscillating_Particle, C4:93-381): history Itr,F_D,F_L (C4:279),
+//   the disk in code, the particle dump named 0_P1_output.txt (C4:342).
+//
+//   lbm_main --case c1|c6|c3|c4 [--nx N] [--ny N] [--steps N] [--input FILE]
 //            [--precision fp64|fp32] [--out DIR] [--fields-every N]
 //            [--dump DIR] [--restart DIR] [--device N] [--chunk N]
 #include <algorithm>
@@ -44,6 +47,7 @@ struct Opts {
   std::string cas = "c1", input = "0_Particle_Initial_Position.txt", out = ".", dump, restart;
   int nx = -1, ny = -1, steps = -1, precision = LBM_FP64, device = 0, fields_every = 0;
   int chunk = 1000;
+  double lc = -1, ret = -1, tc = -1;  // C4 PARAMETER overrides (L_C, RE_T, T_C)
 };
 
 [[noreturn]] void die(const std::string& msg) {
@@ -61,6 +65,7 @@ double r4(double x) { return (double)(float)x; }  // a default-kind REAL literal
 struct Case {
   lbm_params p;
   double c_l = 0, c_t = 0, c_u = 0, c_g = 0, u_c = 1, l_c = 30, rho_s = 1.25, diam = 30;
+  double t_c = 0, f_c = 0;  // C4: oscillation period and force scale
   int np = 1, time_max = 0, time_sample = 0;
   std::vector<double> pin;  // np * LBM_PIN
 };
@@ -148,6 +153,29 @@ Case make_case(const Opts& o) {
     c.time_max = (int)std::lround(r4(1.6) * c.l_c * c.l_c / nu);
     c.np = 1;
     c.pin = {0.5 * (double)p.nx, (double)p.ny - 7.0 * c.l_c, 0, 0, 0, 0, c.l_c, rho_s};
+  } else if (o.cas == "c4") {  // 4_Oscillating_Particle, C4:2-93, C4:197-214
+    p.nx = o.nx > 0 ? o.nx : 1500;
+    p.ny = o.ny > 0 ? o.ny : 1000;
+    const double nu = r4(0.025), re_t = o.ret > 0 ? o.ret : 100.0;
+    c.l_c = o.lc > 0 ? o.lc : 50.0;
+    c.u_c = re_t * nu / c.l_c;                        // C4:30
+    c.t_c = o.tc > 0 ? o.tc : 5.0 * c.l_c / c.u_c;    // C4:32
+    c.f_c = 0.5 * c.u_c * c.u_c * c.l_c;              // C4:33
+    p.nu = nu;
+    p.bc = LBM_BC_EQUILIBRIUM;
+    p.rate_set = LBM_RATES_Q_OF_OMEGA;
+    p.s_e = r4(1.6);
+    p.s_eps = r4(1.8);
+    p.gravity = 0.0;
+    p.wall_model = LBM_WALL_NONE;
+    p.motion = LBM_MOTION_OSCILLATE;
+    p.osc_u = c.u_c;
+    p.osc_period = c.t_c;
+    c.time_max = (int)(6.0 * c.t_c);                  // DO WHILE(KK<INT(6.0*T_C))
+    c.np = 1;
+    c.rho_s = 1.0;
+    c.diam = c.l_c;
+    c.pin = {0.5 * (double)p.nx, 0.5 * (double)p.ny, 0, -c.u_c, 0, 0, c.l_c, 1.0};
   } else if (o.cas == "c3") {  // 3_MultiParticle_Sedimentation, C3:2-83, C3:145-156
     p.nx = o.nx > 0 ? o.nx : 512;
     p.ny = o.ny > 0 ? o.ny : 512;
@@ -265,7 +293,7 @@ void write_dump(lbm_sim* h, const Case& c, const std::string& dir) {
   std::ofstream f51(path_in(dir, "0_F_output.txt")), f52(path_in(dir, "0_UX_output.txt")),
       f53(path_in(dir, "0_UY_output.txt")), f54(path_in(dir, "0_RHO_output.txt")),
       f55(path_in(dir, "0_Gspm_output.txt")), f56(path_in(dir, "0_OmegaBN_output.txt")),
-      f57(path_in(dir, "0_Particle_output.txt")), f59(path_in(dir, "0_OmegaMRT_output.txt"));
+      f57(path_in(dir, c.p.motion == LBM_MOTION_OSCILLATE ? "0_P1_output.txt" : "0_Particle_output.txt")), f59(path_in(dir, "0_OmegaMRT_output.txt"));
   if (!f51 || !f57) die("cannot write the dump into " + dir);
   for (size_t i = 0; i < n1x; ++i)
     for (size_t j = 0; j < n1y; ++j) {
@@ -299,7 +327,7 @@ void read_dump(lbm_sim* h, const Case& c, const std::string& dir) {
   const size_t n1x = p.nx + 1, n1y = p.ny + 1, nn = n1x * n1y;
   const std::vector<double> Fio = read_records(path_in(dir, "0_F_output.txt"), (int)nn, 9);
   const std::vector<double> omio = read_records(path_in(dir, "0_OmegaBN_output.txt"), (int)nn, 1);
-  const std::vector<double> pr = read_records(path_in(dir, "0_Particle_output.txt"), c.np, 8);
+  const std::vector<double> pr = read_records(path_in(dir, c.p.motion == LBM_MOTION_OSCILLATE ? "0_P1_output.txt" : "0_Particle_output.txt"), c.np, 8);
   std::vector<double> F(9 * nn), om(nn), ps((size_t)c.np * LBM_STATE_PER, 0.0);
   size_t r = 0;
   for (size_t i = 0; i < n1x; ++i)
@@ -331,9 +359,10 @@ Opts parse(int argc, char** argv) {
     };
     if (k == "--help" || k == "-h") {
       std::printf(
-          "lbm_main --case c1|c6|c3 [--nx N] [--ny N] [--steps N] [--input FILE]\n"
+          "lbm_main --case c1|c6|c3|c4 [--nx N] [--ny N] [--steps N] [--input FILE]\n"
           "         [--precision fp64|fp32] [--out DIR] [--fields-every N]\n"
-          "         [--dump DIR] [--restart DIR] [--device N] [--chunk N]\n");
+          "         [--dump DIR] [--restart DIR] [--device N] [--chunk N]\n"
+          "         [--lc L_C] [--ret RE_T] [--tc T_C]   (c4 PARAMETERs)\n");
       std::exit(0);
     } else if (k == "--case") o.cas = val();
     else if (k == "--nx") o.nx = std::atoi(val().c_str());
@@ -346,6 +375,9 @@ Opts parse(int argc, char** argv) {
     else if (k == "--device") o.device = std::atoi(val().c_str());
     else if (k == "--fields-every") o.fields_every = std::atoi(val().c_str());
     else if (k == "--chunk") o.chunk = std::max(1, std::atoi(val().c_str()));
+    else if (k == "--lc") o.lc = std::atof(val().c_str());
+    else if (k == "--ret") o.ret = std::atof(val().c_str());
+    else if (k == "--tc") o.tc = std::atof(val().c_str());
     else if (k == "--precision") {
       const std::string v = val();
       if (v == "fp64") o.precision = LBM_FP64;
@@ -388,8 +420,9 @@ int main(int argc, char** argv) {
     f11 << " VARIABLES=T,UX_AVG,UY_AVG,UX_FLC,UY_FLC,PHI,DX,DY\n";
   } else {
     f11.open(path_in(o.out, "01_ParticleTimehistory.plt"));
-    f11 << (o.cas == "c1" ? " VARIABLES=T,Y,Uy,Re_P,E_t\n"
-                          : " VARIABLES=T,Y,X,ANG,Ux,Uy,OMG,Fx,BnT,Cd,ReT\n");
+    f11 << (o.cas == "c1"   ? " VARIABLES=T,Y,Uy,Re_P,E_t\n"
+            : o.cas == "c4" ? " VARIABLES=Itr,F_D,F_L\n"
+                            : " VARIABLES=T,Y,X,ANG,Ux,Uy,OMG,Fx,BnT,Cd,ReT\n");
   }
 
   const auto t0 = std::chrono::steady_clock::now();
@@ -398,6 +431,14 @@ int main(int argc, char** argv) {
   std::vector<double> rec((size_t)len * (o.chunk + 8));
   double er = 1.0;
   long long kk = 0;
+  // C4 writes after the lattice pass (C4:279): the row of step k carries the
+  // force of step k, which the record of step k+1 starts with
+  long long c4_k = -1;
+  double c4_fhx = 0.0;
+  auto c4_row = [&](double fx) {
+    f11 << ' ' << fmt((double)c4_k / c.t_c) << ' ' << fmt((fx + c4_fhx) / c.f_c) << ' '
+        << fmt(fx / c.f_c) << '\n';
+  };
   while (kk < steps) {
     int n = (int)std::min<long long>(o.chunk, steps - kk);
     if (o.fields_every > 0) n = std::min<long long>(n, o.fields_every - kk % o.fields_every);
@@ -413,7 +454,11 @@ int main(int argc, char** argv) {
       if (o.cas == "c3" || c.np < 1) continue;
       const double* d = R + LBM_SERIES_HEAD;  // x y angle u v omega Fx Fy Tz Fin_x Fin_y Fin_t
       const double x = d[0], y = d[1], ang = d[2], u = d[3], v = d[4], w = d[5];
-      if (o.cas == "c1") {  // C1:261-264
+      if (o.cas == "c4") {
+        if (c4_k >= 0) c4_row(d[6]);
+        c4_k = (long long)k;
+        c4_fhx = d[9];
+      } else if (o.cas == "c1") {  // C1:261-264
         const double re_p = c.pin[7] * c.diam * std::sqrt(u * u + v * v) / p.nu;
         const double dp = 0.5 * r4(0.25);  // 0.5*DIAM_PHYSICAL
         const double e_t = 0.5 * (c.rho_s * p.pi * (dp * dp)) * (u * u + v * v) * (c.c_u * c.c_u);
@@ -432,6 +477,11 @@ int main(int argc, char** argv) {
       f7 << ' ' << kk << ' ' << fmt(er) << '\n';
     }
     if (o.fields_every > 0 && kk % o.fields_every == 0) write_fields(h, p, kk, o.out);
+  }
+  if (o.cas == "c4" && c4_k >= 0) {  // the last row: the final state's force
+    std::vector<double> po((size_t)c.np * LBM_POUT);
+    check(lbm_get_particles(h, po.data()), "lbm_get_particles");
+    c4_row(po[6]);
   }
   const double secs =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

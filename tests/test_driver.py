@@ -92,3 +92,20 @@ def test_driver_c1_history_fields_and_restart(pkg, cases, tmp_path):
         np.testing.assert_array_equal(got[0], q[[0, 1, 3, 4, 5, 6, 7, 8]])
     finally:
         sim.close()
+
+
+@pytest.mark.gpu
+def test_driver_c4_history_matches_reference(tmp_path):
+    """lbm_main --case c4 on the C4 fixture's parameters: its
+    01_ParticleTimehistory.plt against the reference's unit 11."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "c4_oscillate.npz"))
+    _run(["--case", "c4", "--nx", "40", "--ny", "30", "--lc", "10", "--ret", "10", "--tc", "40",
+          "--chunk", "64"], tmp_path)
+    hist = _table(tmp_path / "01_ParticleTimehistory.plt")
+    ref = g["UNIT11"]
+    assert hist.shape == ref.shape
+    np.testing.assert_allclose(hist[:, 0], ref[:, 0], rtol=1e-15)
+    scale = np.max(np.abs(ref[:, 1:]))
+    assert np.max(np.abs(hist[:, 1:] - ref[:, 1:])) <= 1e-9 * scale
+    dens = _table(tmp_path / "01_AveragedDensity.PLT")
+    np.testing.assert_allclose(dens, g["UNIT8"], rtol=1e-12)
