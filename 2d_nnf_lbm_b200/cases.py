@@ -125,6 +125,41 @@ def shipped_c6(nx: int = 80, ny: int = 300) -> tuple[LbmParams, np.ndarray]:
     return p, disk
 
 
+def shipped_c2(nx: int = 200, ny: int = 800, l_c: float = 20.0,
+               a_g: float | None = None) -> tuple[LbmParams, np.ndarray]:
+    """2_DKT_Newtonian (C2:2-88, C2:128-144): two disks D = L_C, rho_p =
+    RHO_S = 1.01, at the coded (1/C_L, 7.2/C_L) and (0.97/C_L, 6.8/C_L) with
+    C_L = DIAM_PHYSICAL/L_C; half-way bounce-back with the oscillating-wall
+    amplitude at its shipped zero (C2:1224-1230), Glowinski repulsion with
+    offset walls and the stale D_PW test (C2:735-780), rates 1.1 / 1.25 /
+    q(omega) (C2:1029), angle integration (C2:321).  A_G = -9.81/C_G
+    (C2:33) unless given; returns params and the two disks."""
+    p = LbmParams(nx=nx, ny=ny)
+    nu = r4(0.05)
+    rho_s = r4(1.01)
+    c_l = r4(0.2) / l_c
+    if a_g is None:
+        c_t = (c_l * c_l) * nu / r4(0.01)
+        c_g = c_l * r4(0.01) / (c_t * c_t)
+        a_g = -r4(9.81) / c_g
+    p.nu = nu
+    p.bc = LBM_BC_HALFWAY_BB
+    p.rheology = LBM_NEWTONIAN
+    p.rate_set = LBM_RATES_Q_OF_OMEGA
+    p.s_e, p.s_eps = r4(1.1), 1.25
+    p.wall_model = LBM_WALL_OFFSET
+    p.contact_test = LBM_CONTACT_STALE_DPW
+    p.integrate_angle = 1
+    p.gravity = a_g
+    p.zeta = 1.0
+    p.rep_zeta = 1.0
+    p.eps_p = p.eps_w = 1.0
+    p.e_p = p.e_w = 20.0
+    p.c_ij = glowinski_cij(rho_s, 1.0, a_g, p.pi, l_c)
+    xy = [[r4(1.0) / c_l, r4(7.2) / c_l], [r4(0.97) / c_l, r4(6.8) / c_l]]
+    return p, pin_array(xy, l_c, rho_s)
+
+
 def shipped_c4(nx: int = 1500, ny: int = 1000, l_c: float = 50.0, re_t: float = 100.0,
                t_c: float | None = None) -> tuple[LbmParams, np.ndarray]:
     """4_Oscillating_Particle (C4:2-93, C4:197-214): a cylinder D = L_C,

@@ -21,6 +21,10 @@ named; only PARAMETERs and the particle input file are replaced):
              chain, rate set q(omega), angle integration
   c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
              the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
+  c2_dkt     2_DKT_Newtonian (C2), NX=30 NY=112, L_C=3 (the two disks D=3 at
+             the coded (1/C_L, 7.2/C_L) and (0.97/C_L, 6.8/C_L)), A_G=-5E-4,
+             40 steps: half-way bounce-back, offset-wall repulsion with the
+             stale D_PW test, rates 1.1/1.25/q(omega), angle integration
   c4_oscillate  4_Oscillating_Particle (C4), NX=40 NY=30, L_C=10 (the disk
              D=10 at the centre), RE_T=10 (U_C=0.025), T_C=40 (the loop runs
              INT(6*T_C)=240 steps): prescribed u=-U_C*cos(2*PI*KK/T_C),
@@ -65,6 +69,10 @@ CASES = {
     "c6_bingham": dict(file="6_FreeFall_YieldStress/D2Q9_BinghamSediment_Validated_20191127.f90",
                        overrides={"NX": "24", "NY": "60", "TIME_MAX": "30"},
                        particles=None, steps=30),
+    "c2_dkt": dict(file="2_DKT_Newtonian/D2Q9_DKT_Validated_20190926.f90",
+                   overrides={"NX": "30", "NY": "112", "L_C": "3.0", "TIME_MAX": "40",
+                              "A_G": "-5.0E-4"},
+                   particles=None, steps=40),
     "c4_oscillate": dict(file="4_Oscillating_Particle/D2Q9_V7_OscillatingCylinder_Validated.f90",
                          overrides={"NX": "40", "NY": "30", "L_C": "10.0", "RE_T": "10.0",
                                     "T_C": "40.0"},

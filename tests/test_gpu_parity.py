@@ -316,3 +316,29 @@ def test_c4_checkpoint_roundtrip(pkg, cases):
     assert np.array_equal(a.particles(), b.particles())
     assert np.array_equal(a.field("ux"), b.field("ux"))
     assert np.array_equal(a.field("rho"), b.field("rho"))
+
+
+@pytest.mark.parametrize("precision,rtol", [(0, 1e-10), (1, 2e-4)])
+def test_c2_two_disks_match_reference_golden(pkg, cases, precision, rtol):
+    """Case 2 (DKT, two disks) on the existing kernels against the
+    reference's own run: fields, populations, both disks."""
+    g = _golden("c2_dkt")
+    p, disks = cases.shipped_c2(30, 112, 3.0, float(np.float32(-5.0e-4)))
+    p.precision = precision
+    sim = pkg.Simulation(p)
+    try:
+        sim.set_particles(disks)
+        sim.step(int(g["steps"]))
+        for f, ref in (("ux", g["UX"]), ("uy", g["UY"]), ("gx", g["G"][0]), ("gy", g["G"][1])):
+            close64(sim.field(f).T, ref, rtol, f"field {f}")
+        f, _, _ = sim.get_state()
+        n1x, n1y = p.nx + 1, p.ny + 1
+        close64(f.reshape(n1y, n1x, 9).transpose(2, 1, 0), g["F"], rtol, "F after BC")
+        gp = sim.particles()
+        close64(gp[:, 0:2] - g["DISK_CENTER"][0], g["DISK_CENTER"] - g["DISK_CENTER"][0], 1.0,
+                "centre", scale=max(rtol, 1e-12))
+        close64(gp[:, 3:6], g["DISK_VELOCITY"], rtol, "velocity")
+        close64(gp[:, 6:9], g["DISK_FORCE"], rtol, "force")
+        close64(gp[:, 2], g["DISK_ANGLE"], rtol, "angle")
+    finally:
+        sim.close()

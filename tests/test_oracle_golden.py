@@ -37,13 +37,16 @@ def _setup(cases, name):
                               float(np.float32(1.01)))
         # the reference's D_PW local starts at zero in the translated run
         return p, pin, {"stale_dpw_init": 0.0}
+    if name == "c2_dkt":
+        p, disks = cases.shipped_c2(30, 112, 3.0, float(np.float32(-5.0e-4)))
+        return p, disks, {"stale_dpw_init": 0.0}
     if name == "c4_oscillate":
         p, disk = cases.shipped_c4(40, 30, 10.0, 10.0, 40.0)
         return p, disk, {}
     raise KeyError(name)
 
 
-CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c4_oscillate"]
+CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c2_dkt", "c4_oscillate"]
 
 
 def _exact(a, b, what):
