@@ -647,7 +647,8 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if (p.motion != LBM_MOTION_FREE && p.motion != LBM_MOTION_OSCILLATE) return LBM_E_INVALID;
   if (p.motion == LBM_MOTION_OSCILLATE && (!std::isfinite(p.osc_u) || !(p.osc_period > 0.0)))
     return LBM_E_INVALID;
-  if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM) return LBM_E_INVALID;
+  if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM && p.rheology != LBM_CASSON)
+    return LBM_E_INVALID;
   if (p.wall_model < 0 || p.wall_model > 2 || p.contact_test < 0 || p.contact_test > 1)
     return LBM_E_INVALID;
   if (!std::isfinite(p.nu) || !(p.rho0 > 0.0) || !(p.zeta > 0.0) || !(p.rep_zeta > 0.0) ||
@@ -677,7 +678,8 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   h->g.lty = (p.ny + 1 + LTY - 1) / LTY;
   Model& m = h->m;
   m.bc = p.bc;
-  m.bingham = p.rheology == LBM_BINGHAM;
+  m.bingham = p.rheology == LBM_BINGHAM || p.rheology == LBM_CASSON;
+  m.casson = p.rheology == LBM_CASSON;
   m.q_of_omega = p.rate_set == LBM_RATES_Q_OF_OMEGA;
   m.record_stress = p.record_stress ? 1 : 0;
   m.rho0 = p.rho0;

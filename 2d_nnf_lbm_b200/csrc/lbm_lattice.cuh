@@ -260,10 +260,18 @@ __device__ __forceinline__ void collide_double(const Model& m, double* f, double
     D12 = D12 * INV_RHO;
     const double GAMMA = sqrt(2.0 * fabs(D11 * D11 + D22 * D22 + 2.0 * (D12 * D12)));
     double NU_A;
-    if (GAMMA < m.gamma_min)
+    if (m.casson) {  // C3:985-989
+      if (GAMMA < m.gamma_min) {
+        NU_A = sqrt(NU) + sqrt(m.m_pap * m.tau_y);
+      } else {
+        NU_A = sqrt(NU) + sqrt(m.tau_y / GAMMA) * (1.0 - exp(-sqrt(m.m_pap * GAMMA)));
+        NU_A = NU_A * NU_A;
+      }
+    } else if (GAMMA < m.gamma_min) {
       NU_A = NU + m.m_pap * m.tau_y;
-    else
+    } else {
       NU_A = NU + (m.tau_y / GAMMA) * (1.0 - exp(-(m.m_pap * GAMMA)));
+    }
     no.t11 = NU_A * 2.0 * D11;
     no.t22 = NU_A * 2.0 * D22;
     no.t12 = NU_A * 2.0 * D12;
@@ -373,10 +381,18 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
     const float gam = sqrtf(2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12)));
     const float ty = m.tau_y_f;
     float nua;
-    if (gam < m.gamma_min_f)
+    if (m.casson) {
+      if (gam < m.gamma_min_f) {
+        nua = sqrtf(NU) + sqrtf(m.m_pap_f * ty);
+      } else {
+        nua = sqrtf(NU) + sqrtf(ty / gam) * (1.0f - expf(-sqrtf(m.m_pap_f * gam)));
+        nua = nua * nua;
+      }
+    } else if (gam < m.gamma_min_f) {
       nua = NU + m.m_pap_f * ty;
-    else
+    } else {
       nua = NU + (ty / gam) * (1.0f - expf(-(m.m_pap_f * gam)));
+    }
     const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
     no.t11 = t11;
     no.t22 = t22;

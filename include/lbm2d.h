@@ -63,7 +63,12 @@ enum { LBM_MOTION_FREE = 0,      /* Newton-Euler (C1:247-259)                   
                                     (C4:270-272)                               */ };
 
 enum { LBM_NEWTONIAN = 0,
-       LBM_BINGHAM = 1 };       /* Papanastasiou-regularised, C6:913-958       */
+       LBM_BINGHAM = 1,         /* Papanastasiou-regularised, C6:913-958       */
+       LBM_CASSON = 2 };        /* regularised Casson of the non-Newtonian
+                                   branch of C2/C3 (C3:978-996): the strain
+                                   rate and omega of LBM_BINGHAM, viscosity
+                                   (sqrt(nu) + sqrt(tau_y/g)(1-exp(-sqrt(m g))))^2,
+                                   sqrt(nu) + sqrt(m tau_y) at zero shear    */
 
 enum { LBM_RATES_FIXED_Q = 0,   /* C1:1040-1042: s_q given                     */
        LBM_RATES_Q_OF_OMEGA = 1 /* C6:1009-1011: s_q = 8(2-w)/(8-w)            */ };

@@ -215,15 +215,22 @@ static void collision_node(oracle* o, size_t n, const double* S, double* Fn, dou
     double D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
     double NU = o->p.nu;
     double T11 = NU * 2.0 * D11, T22 = NU * 2.0 * D22, T12 = NU * 2.0 * D12; /* C6:918 */
-    if (o->p.rheology == LBM_BINGHAM) {
-        /* C6:921-958 */
+    if (o->p.rheology == LBM_BINGHAM || o->p.rheology == LBM_CASSON) {
+        /* C6:921-958; Casson C3:978-996 */
         double INV_RHO = 1.0 / RHO;
         D11 = D11 * INV_RHO;
         D22 = D22 * INV_RHO;
         D12 = D12 * INV_RHO;
         double GAMMA = sqrt(2.0 * fabs(D11 * D11 + D22 * D22 + 2.0 * (D12 * D12)));
         double NU_A;
-        if (GAMMA < o->p.gamma_min)
+        if (o->p.rheology == LBM_CASSON) {
+            if (GAMMA < o->p.gamma_min)
+                NU_A = sqrt(NU) + sqrt(o->p.m_pap * o->p.tau_y);
+            else {
+                NU_A = sqrt(NU) + sqrt(o->p.tau_y / GAMMA) * (1.0 - exp(-sqrt(o->p.m_pap * GAMMA)));
+                NU_A = NU_A * NU_A;
+            }
+        } else if (GAMMA < o->p.gamma_min)
             NU_A = NU + o->p.m_pap * o->p.tau_y;
         else
             NU_A = NU + (o->p.tau_y / GAMMA) * (1.0 - exp(-(o->p.m_pap * GAMMA)));
@@ -242,7 +249,7 @@ static void collision_node(oracle* o, size_t n, const double* S, double* Fn, dou
 
 static void collision_mrt(oracle* o) {
     double S[Q];
-    int bingham = o->p.rheology == LBM_BINGHAM;
+    int bingham = o->p.rheology == LBM_BINGHAM || o->p.rheology == LBM_CASSON;
     for (int j = 0; j <= o->ny; ++j)
         for (int i = 0; i <= o->nx; ++i) {
             size_t n = IDX(o, i, j);

@@ -21,6 +21,9 @@ named; only PARAMETERs and the particle input file are replaced):
              chain, rate set q(omega), angle integration
   c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
              the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
+  c3_casson  C3 as c3_multi with its non-Newtonian branch switched on
+             (NON_NEWTONIAN=.TRUE., Y_g=0.5): the regularised Casson
+             viscosity of C3:978-996 with the node-to-node omega chain
   c2_dkt     2_DKT_Newtonian (C2), NX=30 NY=112, L_C=3 (the two disks D=3 at
              the coded (1/C_L, 7.2/C_L) and (0.97/C_L, 6.8/C_L)), A_G=-5E-4,
              40 steps: half-way bounce-back, offset-wall repulsion with the
@@ -69,6 +72,10 @@ CASES = {
     "c6_bingham": dict(file="6_FreeFall_YieldStress/D2Q9_BinghamSediment_Validated_20191127.f90",
                        overrides={"NX": "24", "NY": "60", "TIME_MAX": "30"},
                        particles=None, steps=30),
+    "c3_casson": dict(file="3_MultiParticle_Sedimentation/D2Q9_RTParticle_20191003.f90",
+                      overrides={"NX": "48", "NY": "72", "TIME_MAX": "20", "N_PARTICLE": "3",
+                                 "NON_NEWTONIAN": ".TRUE.", "Y_g": "0.5"},
+                      particles="\t\n14\t50\n30.6\t50\n24\t22\n", steps=20, skip_lines=[202]),
     "c2_dkt": dict(file="2_DKT_Newtonian/D2Q9_DKT_Validated_20190926.f90",
                    overrides={"NX": "30", "NY": "112", "L_C": "3.0", "TIME_MAX": "40",
                               "A_G": "-5.0E-4"},

@@ -116,6 +116,23 @@ def test_c6_bingham_fp64(pkg, cases, bc):
     assert np.mean(gi != ri) < 1e-3
 
 
+def test_c3_casson_fp64(pkg, cases):
+    """The Casson viscosity of C3's non-Newtonian branch (C3:978-996),
+    three disks, per-node omega of the previous step."""
+    p = cases.shipped_c3(48, 72)
+    p.rheology = 2  # LBM_CASSON
+    p.tau_y = 0.5 * (float(np.float32(1.01)) - 1.0) * (-p.gravity) * 16.0
+    p.m_pap = float(np.float32(1.0e6))
+    p.record_stress = 1
+    pin = cases.pin_array([[14.0, 50.0], [30.6, 50.0], [24.0, 22.0]], 16.0,
+                          float(np.float32(1.01)))
+    sim, ref = pair(pkg, p, pin, 60)
+    compare_all(sim, ref, rtol=1e-8)
+    close64(sim.field("omega"), ref.field("omega"), 1e-8, "omega")
+    for f in ("tau11", "tau22", "tau12"):
+        close64(sim.field(f), ref.field(f), 1e-8, f)
+
+
 @pytest.mark.parametrize("contact", [0, 1])
 def test_multiparticle_fp64(pkg, cases, contact):
     rng = np.random.default_rng(3)

@@ -37,6 +37,14 @@ def _setup(cases, name):
                               float(np.float32(1.01)))
         # the reference's D_PW local starts at zero in the translated run
         return p, pin, {"stale_dpw_init": 0.0}
+    if name == "c3_casson":
+        p = cases.shipped_c3(48, 72)
+        p.rheology = 2  # LBM_CASSON
+        p.tau_y = 0.5 * (float(np.float32(1.01)) - 1.0) * (-p.gravity) * 16.0  # C3:48
+        p.m_pap = float(np.float32(1.0e6))
+        pin = cases.pin_array([[14.0, 50.0], [30.6, 50.0], [24.0, 22.0]], 16.0,
+                              float(np.float32(1.01)))
+        return p, pin, {"stale_dpw_init": 0.0, "omega_chain": 1}
     if name == "c2_dkt":
         p, disks = cases.shipped_c2(30, 112, 3.0, float(np.float32(-5.0e-4)))
         return p, disks, {"stale_dpw_init": 0.0}
@@ -46,7 +54,7 @@ def _setup(cases, name):
     raise KeyError(name)
 
 
-CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c2_dkt", "c4_oscillate"]
+CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c3_casson", "c2_dkt", "c4_oscillate"]
 
 
 def _exact(a, b, what):
@@ -75,7 +83,7 @@ def test_oracle_reproduces_reference_bit_for_bit(cases, name):
         _exact(o.field("rho").T, g["RHO"], "RHO")
         _exact(o.field("gx").T, g["G"][0], "G(1)")
         _exact(o.field("gy").T, g["G"][1], "G(2)")
-        if "OMEGA_BN" in g and p.rheology == 1:
+        if "OMEGA_BN" in g and p.rheology in (1, 2):  # Bingham, Casson
             _exact(o.field("omega").T, g["OMEGA_BN"], "OMEGA_BN")
         op = o.particles()
         _exact(op[:, 0:2], g["DISK_CENTER"], "CENTER")
