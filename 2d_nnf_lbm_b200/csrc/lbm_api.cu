@@ -645,6 +645,7 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if (p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB && p.bc != LBM_BC_EQUILIBRIUM)
     return LBM_E_INVALID;
   if (p.motion != LBM_MOTION_FREE && p.motion != LBM_MOTION_OSCILLATE) return LBM_E_INVALID;
+  if (p.strain_model != LBM_STRAIN_MEQ && p.strain_model != LBM_STRAIN_FEQ) return LBM_E_INVALID;
   if (p.motion == LBM_MOTION_OSCILLATE && (!std::isfinite(p.osc_u) || !(p.osc_period > 0.0)))
     return LBM_E_INVALID;
   if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM && p.rheology != LBM_CASSON)
@@ -680,6 +681,7 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   m.bc = p.bc;
   m.bingham = p.rheology == LBM_BINGHAM || p.rheology == LBM_CASSON;
   m.casson = p.rheology == LBM_CASSON;
+  m.strain_feq = p.strain_model == LBM_STRAIN_FEQ;
   m.q_of_omega = p.rate_set == LBM_RATES_Q_OF_OMEGA;
   m.record_stress = p.record_stress ? 1 : 0;
   m.rho0 = p.rho0;

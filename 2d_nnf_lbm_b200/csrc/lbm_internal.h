@@ -90,6 +90,7 @@ struct Model {
   int bc;            // LBM_BC_*
   int bingham;       // 1: per-node viscosity (Papanastasiou Bingham or Casson)
   int casson;        // 1: the Casson viscosity function
+  int strain_feq;    // 1: strain rate of C1 (m_neq against COMPUTEFEQNEW's moments)
   int q_of_omega;    // 1: s_q = 8(2-w)/(8-w)
   int record_stress; // 1: write stress/yield ring
   double rho0, nu, omega, s_e, s_eps, s_q, d_mrt, pi, zeta;

@@ -223,8 +223,22 @@ __device__ __forceinline__ void collide_double(const Model& m, double* f, double
   if (!want_stress) return;
   // Chai strain rate from S*(m - m_eq) + forcing correction, C6:903-916
   double MNE[9], F1[9];
+  if (m.strain_feq) {  // C1:896-908: against the moments of COMPUTEFEQNEW
+    double FE[9];
+    feq_double(m, UX, UY, RHO, FE);
+    MNE[0] = M[0] - (FE[0] + FE[1] + FE[2] + FE[3] + FE[4] + FE[5] + FE[6] + FE[7] + FE[8]);
+    MNE[1] = M[1] - (-4.0 * FE[0] - FE[1] - FE[2] - FE[3] - FE[4] + 2.0 * (FE[5] + FE[6] + FE[7] + FE[8]));
+    MNE[2] = M[2] - (4.0 * FE[0] - 2.0 * (FE[1] + FE[2] + FE[3] + FE[4]) + (FE[5] + FE[6] + FE[7] + FE[8]));
+    MNE[3] = M[3] - (FE[1] - FE[3] + FE[5] - FE[6] - FE[7] + FE[8]);
+    MNE[4] = M[4] - (-2.0 * (FE[1] - FE[3]) + FE[5] - FE[6] - FE[7] + FE[8]);
+    MNE[5] = M[5] - (FE[2] - FE[4] + FE[5] + FE[6] - FE[7] - FE[8]);
+    MNE[6] = M[6] - (-2.0 * (FE[2] - FE[4]) + FE[5] + FE[6] - FE[7] - FE[8]);
+    MNE[7] = M[7] - (FE[1] - FE[2] + FE[3] - FE[4]);
+    MNE[8] = M[8] - (FE[5] - FE[6] + FE[7] - FE[8]);
+  } else {
 #pragma unroll
-  for (int k = 0; k < 9; ++k) MNE[k] = M[k] - MEQ[k];
+    for (int k = 0; k < 9; ++k) MNE[k] = M[k] - MEQ[k];
+  }
   F1[1] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] -
           6.0 * S[4] * MNE[4] + 9.0 * S[7] * MNE[7];
   F1[2] = 4.0 * S[0] * MNE[0] - 1.0 * S[1] * MNE[1] - 2.0 * S[2] * MNE[2] + 6.0 * S[5] * MNE[5] -
@@ -241,12 +255,25 @@ __device__ __forceinline__ void collide_double(const Model& m, double* f, double
           3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] + 9.0 * S[8] * MNE[8];
   F1[8] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] +
           3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] - 9.0 * S[8] * MNE[8];
-  const double ZARIB = -1.5 * d_mrt;
-  double D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]) +
-               0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
-  double D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]) +
-               0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
-  double D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
+  double D11, D22, D12;
+  if (m.strain_feq) {  // C1:940-948: 1/RHO folded into both terms
+    const double IR = 1.0 / RHO;
+    double ZARIB = -1.5 * d_mrt * IR;
+    D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]);
+    D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]);
+    D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]);
+    ZARIB = 0.75 * IR;
+    D11 = D11 + ZARIB * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
+    D22 = D22 + ZARIB * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
+    D12 = D12 + ZARIB * (-S[7] * (GX * UY + GY * UX));
+  } else {  // C6:903-916
+    const double ZARIB = -1.5 * d_mrt;
+    D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]) +
+          0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
+    D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]) +
+          0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
+    D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
+  }
   const double NU = m.nu;
   no.t11 = NU * 2.0 * D11;
   no.t22 = NU * 2.0 * D22;
@@ -255,9 +282,11 @@ __device__ __forceinline__ void collide_double(const Model& m, double* f, double
   no.omega = S[7];
   if (m.bingham) {
     const double INV_RHO = 1.0 / RHO;
-    D11 = D11 * INV_RHO;
-    D22 = D22 * INV_RHO;
-    D12 = D12 * INV_RHO;
+    if (!m.strain_feq) {
+      D11 = D11 * INV_RHO;
+      D22 = D22 * INV_RHO;
+      D12 = D12 * INV_RHO;
+    }
     const double GAMMA = sqrt(2.0 * fabs(D11 * D11 + D22 * D22 + 2.0 * (D12 * D12)));
     double NU_A;
     if (m.casson) {  // C3:985-989
@@ -367,6 +396,13 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
   float D11 = -d * (t1 + t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gx * ux));
   float D22 = -d * (t1 - t7) + 0.75f * ((r.sw - r.s1) * gu - r.sw * (2.0f * gy * uy));
   float D12 = -54.0f * d * r.sw * n8 + 0.75f * (-r.sw * (gx * uy + gy * ux));
+  if (m.strain_feq) {  // C1:940-948 divides both terms by rho (FP32: the
+    // moments of COMPUTEFEQNEW equal the moment-space equilibrium here)
+    const float ir = 1.0f / rho;
+    D11 *= ir;
+    D22 *= ir;
+    D12 *= ir;
+  }
   const float NU = m.nu_f;
   no.t11 = NU * 2.0f * D11;
   no.t22 = NU * 2.0f * D22;
@@ -375,9 +411,11 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
   no.omega = r.sw;
   if (m.bingham) {
     const float inv_rho = 1.0f / rho;
-    D11 *= inv_rho;
-    D22 *= inv_rho;
-    D12 *= inv_rho;
+    if (!m.strain_feq) {
+      D11 *= inv_rho;
+      D22 *= inv_rho;
+      D12 *= inv_rho;
+    }
     const float gam = sqrtf(2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12)));
     const float ty = m.tau_y_f;
     float nua;

@@ -37,6 +37,7 @@ ERRORS = {
 LBM_FP64, LBM_FP32_SHIFTED = 0, 1
 LBM_BC_ZOUHE, LBM_BC_HALFWAY_BB, LBM_BC_EQUILIBRIUM = 0, 1, 2
 LBM_MOTION_FREE, LBM_MOTION_OSCILLATE = 0, 1
+LBM_STRAIN_MEQ, LBM_STRAIN_FEQ = 0, 1
 LBM_NEWTONIAN, LBM_BINGHAM, LBM_CASSON = 0, 1, 2
 LBM_RATES_FIXED_Q, LBM_RATES_Q_OF_OMEGA = 0, 1
 LBM_WALL_MIRROR, LBM_WALL_OFFSET, LBM_WALL_NONE = 0, 1, 2
@@ -108,6 +109,8 @@ class LbmParams(ctypes.Structure):
         ("wall_mirror_left", ctypes.c_double),
         ("osc_u", ctypes.c_double),
         ("osc_period", ctypes.c_double),
+        ("strain_model", ctypes.c_int32),
+        ("reserved1", ctypes.c_int32),
     ]
 
     def __init__(self, **kw):

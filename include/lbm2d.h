@@ -73,6 +73,11 @@ enum { LBM_NEWTONIAN = 0,
 enum { LBM_RATES_FIXED_Q = 0,   /* C1:1040-1042: s_q given                     */
        LBM_RATES_Q_OF_OMEGA = 1 /* C6:1009-1011: s_q = 8(2-w)/(8-w)            */ };
 
+enum { LBM_STRAIN_MEQ = 0,       /* C6:903-922: m_neq against the moment-space
+                                    equilibrium, forcing correction, then 1/rho */
+       LBM_STRAIN_FEQ = 1 };     /* C1:896-948: m_neq against the moments of
+                                    COMPUTEFEQNEW, 1/rho folded into both terms */
+
 enum { LBM_WALL_MIRROR = 0,     /* C1:737-745: mirror-image wall particles     */
        LBM_WALL_OFFSET = 1,     /* C3:775-783, C6:717-725: wall disk at R out  */
        LBM_WALL_NONE = 2 };
@@ -124,6 +129,8 @@ typedef struct lbm_params {
     double wall_mirror_left;  /* 2*WALL%EDGE(4) (C1:743)                       */
     double osc_u;             /* U_C of LBM_MOTION_OSCILLATE (C4:30)           */
     double osc_period;        /* T_C of LBM_MOTION_OSCILLATE (C4:32)           */
+    int32_t strain_model;     /* LBM_STRAIN_* (non-Newtonian strain rate)      */
+    int32_t reserved1;
 } lbm_params;
 
 /* Particle input record (lbm_set_particles): LBM_PIN doubles per disk. */

@@ -168,8 +168,24 @@ static void collision_node(oracle* o, size_t n, const double* S, double* Fn, dou
     MEQ[6] = RHO * (-UY);
     MEQ[7] = RHO * (UX * UX - UY * UY);
     MEQ[8] = RHO * (UX * UY);
-    /* C6:889 */
-    for (int k = 0; k < Q; ++k) MNE[k] = M[k] - MEQ[k];
+    /* C6:889; LBM_STRAIN_FEQ: against the moments of COMPUTEFEQNEW, C1:896-908 */
+    const int feq_neq = o->p.strain_model == LBM_STRAIN_FEQ;
+    if (feq_neq) {
+        double FE[Q], ME[Q];
+        compute_feq(o, UX, UY, RHO, FE);
+        ME[0] = FE[0] + FE[1] + FE[2] + FE[3] + FE[4] + FE[5] + FE[6] + FE[7] + FE[8];
+        ME[1] = -4.0 * FE[0] - FE[1] - FE[2] - FE[3] - FE[4] + 2.0 * (FE[5] + FE[6] + FE[7] + FE[8]);
+        ME[2] = 4.0 * FE[0] - 2.0 * (FE[1] + FE[2] + FE[3] + FE[4]) + (FE[5] + FE[6] + FE[7] + FE[8]);
+        ME[3] = FE[1] - FE[3] + FE[5] - FE[6] - FE[7] + FE[8];
+        ME[4] = -2.0 * (FE[1] - FE[3]) + FE[5] - FE[6] - FE[7] + FE[8];
+        ME[5] = FE[2] - FE[4] + FE[5] + FE[6] - FE[7] - FE[8];
+        ME[6] = -2.0 * (FE[2] - FE[4]) + FE[5] + FE[6] - FE[7] - FE[8];
+        ME[7] = FE[1] - FE[2] + FE[3] - FE[4];
+        ME[8] = FE[5] - FE[6] + FE[7] - FE[8];
+        for (int k = 0; k < Q; ++k) MNE[k] = M[k] - ME[k];
+    } else {
+        for (int k = 0; k < Q; ++k) MNE[k] = M[k] - MEQ[k];
+    }
     /* C1:911 */
     double m[Q];
     for (int k = 0; k < Q; ++k)
@@ -207,20 +223,35 @@ static void collision_node(oracle* o, size_t n, const double* S, double* Fn, dou
             3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] + 9.0 * S[8] * MNE[8];
     F1[8] = 4.0 * S[0] * MNE[0] + 2.0 * S[1] * MNE[1] + 1.0 * S[2] * MNE[2] + 6.0 * S[3] * MNE[3] +
             3.0 * S[4] * MNE[4] - 6.0 * S[5] * MNE[5] - 3.0 * S[6] * MNE[6] - 9.0 * S[8] * MNE[8];
-    double ZARIB = -1.5 * d_mrt;
-    double D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]) +
-                 0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
-    double D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]) +
-                 0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
-    double D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
+    double D11, D22, D12;
+    if (feq_neq) { /* C1:940-948: 1/RHO folded into both terms */
+        double IR = 1.0 / RHO;
+        double ZARIB = -1.5 * d_mrt * IR;
+        D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]);
+        D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]);
+        D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]);
+        ZARIB = 0.75 * IR;
+        D11 = D11 + ZARIB * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
+        D22 = D22 + ZARIB * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
+        D12 = D12 + ZARIB * (-S[7] * (GX * UY + GY * UX));
+    } else { /* C6:903-916 */
+        double ZARIB = -1.5 * d_mrt;
+        D11 = ZARIB * (F1[1] + F1[5] + F1[6] + F1[3] + F1[7] + F1[8]) +
+              0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GX * UX));
+        D22 = ZARIB * (F1[5] + F1[2] + F1[6] + F1[7] + F1[4] + F1[8]) +
+              0.75 * ((S[7] - S[1]) * (GX * UX + GY * UY) - S[7] * (2.0 * GY * UY));
+        D12 = ZARIB * (F1[5] - F1[6] + F1[7] - F1[8]) + 0.75 * (-S[7] * (GX * UY + GY * UX));
+    }
     double NU = o->p.nu;
     double T11 = NU * 2.0 * D11, T22 = NU * 2.0 * D22, T12 = NU * 2.0 * D12; /* C6:918 */
     if (o->p.rheology == LBM_BINGHAM || o->p.rheology == LBM_CASSON) {
         /* C6:921-958; Casson C3:978-996 */
         double INV_RHO = 1.0 / RHO;
-        D11 = D11 * INV_RHO;
-        D22 = D22 * INV_RHO;
-        D12 = D12 * INV_RHO;
+        if (!feq_neq) {
+            D11 = D11 * INV_RHO;
+            D22 = D22 * INV_RHO;
+            D12 = D12 * INV_RHO;
+        }
         double GAMMA = sqrt(2.0 * fabs(D11 * D11 + D22 * D22 + 2.0 * (D12 * D12)));
         double NU_A;
         if (o->p.rheology == LBM_CASSON) {

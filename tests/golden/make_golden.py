@@ -19,6 +19,10 @@ named; only PARAMETERs and the particle input file are replaced):
              disk at its coded start (12, 18)), 30 steps: half-way
              bounce-back, Papanastasiou viscosity with the node-to-node omega
              chain, rate set q(omega), angle integration
+  c1_nonnewt C1 as c1_center with its non-Newtonian branch switched on
+             (NON_NEWTONIAN=.TRUE.): Papanastasiou viscosity with the strain
+             rate of C1:896-948 (m_neq against COMPUTEFEQNEW's moments) and
+             the node-to-node omega chain
   c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
              the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
   c3_casson  C3 as c3_multi with its non-Newtonian branch switched on
@@ -66,6 +70,9 @@ CASES = {
     "c1_walls": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
                      overrides={"NX": "24", "NY": "40", "TIME_MAX": "20"},
                      particles="19.02\t4.98\t8\t1.25", steps=20),
+    "c1_nonnewt": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
+                       overrides={"NX": "24", "NY": "40", "TIME_MAX": "40", "NON_NEWTONIAN": ".TRUE."},
+                       particles="12\t28\t8\t1.25", steps=40),
     "c1_error": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
                      overrides={"NX": "16", "NY": "24", "TIME_MAX": "2000"},
                      particles="8\t14\t6\t1.25", steps=2000),

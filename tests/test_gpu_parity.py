@@ -116,6 +116,22 @@ def test_c6_bingham_fp64(pkg, cases, bc):
     assert np.mean(gi != ri) < 1e-3
 
 
+def test_c1_nonnewtonian_strain_feq_fp64(pkg, cases):
+    """C1's non-Newtonian branch: Papanastasiou viscosity with the strain
+    rate from m - m_eq(COMPUTEFEQNEW) (C1:896-948), per-node omega."""
+    p = cases.shipped_c1(40, 60, 10.0)
+    p.rheology = 1
+    p.strain_model = 1
+    p.record_stress = 1
+    sim, ref = pair(pkg, p, cases.pin_array([[20.0, 40.0]], 10.0, 1.25), 80)
+    compare_all(sim, ref, rtol=1e-8)
+    close64(sim.field("omega"), ref.field("omega"), 1e-8, "omega")
+    # C1's m = 1e8 (18x C6's) amplifies the ulp-level sin() differences
+    # further in the stresses, which scale with the apparent viscosity
+    for f in ("tau11", "tau22", "tau12"):
+        close64(sim.field(f), ref.field(f), 1e-7, f)
+
+
 def test_c3_casson_fp64(pkg, cases):
     """The Casson viscosity of C3's non-Newtonian branch (C3:978-996),
     three disks, per-node omega of the previous step."""

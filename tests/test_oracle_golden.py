@@ -37,6 +37,11 @@ def _setup(cases, name):
                               float(np.float32(1.01)))
         # the reference's D_PW local starts at zero in the translated run
         return p, pin, {"stale_dpw_init": 0.0}
+    if name == "c1_nonnewt":
+        p = cases.shipped_c1(24, 40, 8.0)
+        p.rheology = 1        # LBM_BINGHAM (Papanastasiou, C1:950-954)
+        p.strain_model = 1    # LBM_STRAIN_FEQ (C1:896-948)
+        return p, cases.pin_array([[12.0, 28.0]], 8.0, 1.25), {"omega_chain": 1}
     if name == "c3_casson":
         p = cases.shipped_c3(48, 72)
         p.rheology = 2  # LBM_CASSON
@@ -54,7 +59,7 @@ def _setup(cases, name):
     raise KeyError(name)
 
 
-CASES = ["c1_center", "c1_walls", "c6_bingham", "c3_multi", "c3_casson", "c2_dkt", "c4_oscillate"]
+CASES = ["c1_center", "c1_walls", "c1_nonnewt", "c6_bingham", "c3_multi", "c3_casson", "c2_dkt", "c4_oscillate"]
 
 
 def _exact(a, b, what):
