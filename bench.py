@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the FP32-vs-FP64 trajectory comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="target CPU time of the bounded oracle sample")
     ap.add_argument("--nx", type=int, default=1024)
@@ -260,6 +262,34 @@ def run_e2e(pkg, torch, args, device):
     }
 
 
+def trajectory_error(pkg, args, device, steps):
+    """FP32-shifted against FP64 plain on the bench workload, outside the
+    timed region: the largest disk displacement error after `steps` steps
+    relative to the largest FP64 displacement, and the same for the velocity
+    (the FP64 path matches the oracle within 1e-10 on the parity cases)."""
+    res = {}
+    pin = None
+    for prec in (1, 0):
+        p, pin = workload(pkg, prec, args)
+        p.device = device
+        sim = pkg.Simulation(p)
+        sim.set_particles(pin)
+        sim.step(steps)
+        res[prec] = sim.particles()
+        sim.close()
+    d32, d64 = res[1][:, 0:2] - pin[:, 0:2], res[0][:, 0:2] - pin[:, 0:2]
+    v32, v64 = res[1][:, 3:5], res[0][:, 3:5]
+    tiny = 1e-300
+    return {
+        "steps": steps,
+        "max_rel_displacement_err": float(np.max(np.linalg.norm(d32 - d64, axis=1)) /
+                                          max(float(np.max(np.linalg.norm(d64, axis=1))), tiny)),
+        "max_rel_velocity_err": float(np.max(np.linalg.norm(v32 - v64, axis=1)) /
+                                      max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)),
+        "tolerance": 1e-4,
+    }
+
+
 def cpu_baseline(pkg, args, seconds):
     """The oracle (reference loop structure, one thread) on the same workload,
     timed over a bounded number of whole time steps."""
@@ -392,6 +422,8 @@ def main():
         "status": {"fp32": r32["status"], "fp64": r64["status"],
                    "finite": r32["finite"] and r64["finite"]},
     }
+    if args.accuracy_steps > 0:
+        line["trajectory_err"] = trajectory_error(pkg, args, device, args.accuracy_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pkg, args, args.cpu_seconds)
     if rank == 0:
