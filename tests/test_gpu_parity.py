@@ -374,3 +374,54 @@ def test_c2_two_disks_match_reference_golden(pkg, cases, precision, rtol):
         close64(gp[:, 2], g["DISK_ANGLE"], rtol, "angle")
     finally:
         sim.close()
+
+
+def test_full_size_fp32_trajectory_within_1e4(pkg, cases):
+    """The throughput workload at its full size (1024 x 2048 cells, 512 disks,
+    tau 0.7): FP32-shifted against FP64 plain after 2000 steps, every disk's
+    displacement and velocity within 1e-4 of the largest FP64 value.  The
+    oracle cannot run this size in seconds; FP64 is pinned to it above."""
+    res, pin = {}, None
+    for prec in (1, 0):
+        p, pin = cases.workload_cfg2(prec, 1024, 2048, 512)
+        sim = pkg.Simulation(p)
+        sim.set_particles(pin)
+        sim.step(2000)
+        res[prec] = sim.particles()
+        sim.close()
+    d32, d64 = res[1][:, 0:2] - pin[:, 0:2], res[0][:, 0:2] - pin[:, 0:2]
+    assert np.max(np.linalg.norm(d64, axis=1)) > 1.0  # the disks have moved
+    err = np.max(np.linalg.norm(d32 - d64, axis=1))
+    assert err <= 1e-4 * np.max(np.linalg.norm(d64, axis=1)), err
+    v32, v64 = res[1][:, 3:5], res[0][:, 3:5]
+    verr = np.max(np.linalg.norm(v32 - v64, axis=1))
+    assert verr <= 1e-4 * np.max(np.linalg.norm(v64, axis=1)), verr
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_full_size_checkpoint_roundtrip(pkg, cases, precision):
+    """Restart at the full workload size: a run resumed from a state dump
+    matches the uninterrupted run, bit for bit in FP64.  The FP32 dump holds
+    f = h + w_k rho0 in double, so an h below 2^-54 in magnitude can lose
+    bits on the way back; there the check is 1e-6 of each quantity's scale."""
+    p, pin = cases.workload_cfg2(precision, 1024, 2048, 512)
+    a = pkg.Simulation(p)
+    a.set_particles(pin)
+    a.step(200)
+    f, om, parts = a.get_state()
+    a.step(100)
+    b = pkg.Simulation(p)
+    b.set_state(200, f, om, parts)
+    b.step(100)
+    if precision == 0:
+        assert np.array_equal(a.particles(), b.particles())
+        for name in ("ux", "uy", "rho"):
+            assert np.array_equal(a.field(name), b.field(name)), name
+    else:
+        pa, pb = a.particles(), b.particles()
+        close64(pb[:, 0:2], pa[:, 0:2], 1e-6, "position")
+        close64(pb[:, 3:5], pa[:, 3:5], 1e-6, "velocity")
+        for name in ("ux", "uy", "rho"):
+            close64(b.field(name), a.field(name), 1e-6, name)
+    a.close()
+    b.close()
