@@ -11,6 +11,7 @@ or no CUDA device is present, the calls raise.
 
 from .lbm2d import (  # noqa: F401
     LbmError,
+    LbmObjective,
     LbmParams,
     Simulation,
     library_path,

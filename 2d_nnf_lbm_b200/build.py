@@ -29,6 +29,7 @@ SOURCES = {
     "lbm_fp32.cu": ["--fmad=true"],
     "lbm_particles.cu": ["--fmad=false"],
     "lbm_api.cu": [],
+    "lbm_adjoint.cu": ["--fmad=true"],
     "lbm_noalloc.cu": ["--fmad=false"],
 }
 

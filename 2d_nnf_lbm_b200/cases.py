@@ -318,6 +318,28 @@ def workload_cfg3(precision: int, bn: float, nx=800, ny=2400, diam=40.0) -> tupl
     return p, disk, {"u_ref": u_ref, "bn": bn}
 
 
+def workload_cfg5(precision: int, bn: float = 5.0, nx=400, ny=1200, diam=24.0,
+                  rho_s=1.5) -> tuple[LbmParams, np.ndarray, dict]:
+    """Adjoint workload: the C6 program at 400x1200, one disk D=24 rho_p=1.5,
+    tau_p=0.9, m=1e5, Bingham number Bn; the objective is the disk's mean v_y
+    over steps 3000..4000.  Gravity, velocity scale and Bn follow the
+    viscoplastic-settling workload: A_G = -RE_S*NU^2/(D^3 (rho_s-1)),
+    U_REF = D^2 (rho_s-1)(-A_G)/NU, TAU_Y = Bn*NU*U_REF/D."""
+    p, _ = shipped_c6(nx, ny)
+    p.precision = precision
+    nu = r4((0.9 - 0.5) / 3.0)
+    re_s = r4(0.78)
+    a_g = -(re_s * nu * nu / ((diam ** 3) * (rho_s - 1.0) * 1.0))
+    u_ref = diam * diam * (rho_s - 1.0) * (-a_g) / nu
+    p.nu = nu
+    p.gravity = a_g
+    p.tau_y = bn * nu * u_ref / diam
+    p.m_pap = 1.0e5
+    p.c_ij = glowinski_cij(rho_s, 1.0, a_g, p.pi, diam)
+    disk = pin_array([[0.5 * nx, float(ny) - 7.0 * diam]], diam, rho_s)
+    return p, disk, {"u_ref": u_ref, "bn": bn, "n0": 3000, "n1": 4000}
+
+
 def mlups(nodes: int, steps: int, seconds: float) -> float:
     return nodes * steps / seconds / 1e6
 
@@ -337,6 +359,7 @@ __all__ = [
     "workload_cfg2",
     "workload_cfg2_particles",
     "workload_cfg3",
+    "workload_cfg5",
     "mlups",
     "nodes_of",
 ]

@@ -88,6 +88,23 @@ struct lbm_sim {
   size_t ev_used = 0;
   double prof_ms[2] = {0.0, 0.0};
   int64_t prof_n[2] = {0, 0};
+  // adjoint sweep (lbm_adjoint), allocated on first use and kept
+  unsigned char* adj_slots = nullptr;  // [nslots][10 planes]: f*(n) then omega(n)
+  int adj_nslots = 0;
+  std::vector<CUtensorMap> adj_tm;     // TMA descriptor of each slot's f*
+  unsigned char* adj_ck = nullptr;     // [nck][10 planes] checkpoints
+  int adj_nck = 0;
+  double* adj_ckp = nullptr;           // [nck+1][ckp_len]: records, FORCE sums, D_PW
+  double* adj_hist = nullptr;          // [nhist][PS][npad] particle records of every step
+  long long adj_nhist = 0;
+  void* adj_a[2] = {nullptr, nullptr};  // dJ/dF, T[9 planes]
+  void* adj_w[2] = {nullptr, nullptr};  // dJ/domega, T[plane]
+  double* adj_state = nullptr;         // [8][npad]
+  double* adj_p = nullptr;             // [5][npad]
+  double* adj_h = nullptr;             // [3][npad]
+  double* adj_rho = nullptr;           // [npad]
+  double* adj_g = nullptr;             // [blocks][2]
+  int adj_npad = 0;
 };
 
 namespace {
@@ -469,7 +486,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int make_tensor_maps(lbm_sim* h) {
+// TMA descriptor of the step kernel's reads from the population buffer at base.
+int encode_f_map(const lbm_sim* h, void* base, CUtensorMap* out) {
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -483,13 +501,17 @@ int make_tensor_maps(lbm_sim* h) {
   const cuuint32_t box[3] = {(cuuint32_t)step_box_width((int)h->esz),
                              (cuuint32_t)step_box_rows((int)h->esz), 3};
   const cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(out, h->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                   3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LBM_OK : LBM_E_CUDA;
+}
+
+int make_tensor_maps(lbm_sim* h) {
   for (int b = 0; b < 2; ++b) {
-    CUresult r = enc(&h->tm[b],
-                     h->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                     3, h->f[b], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return LBM_E_CUDA;
+    int rc = encode_f_map(h, h->f[b], &h->tm[b]);
+    if (rc) return rc;
   }
   return LBM_OK;
 }
@@ -511,6 +533,12 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->d_kk); dfree(h->stale_dpw);
   dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
   dfree(h->u0); dfree(h->err_part);
+  dfree(h->adj_slots); dfree(h->adj_ck); dfree(h->adj_ckp); dfree(h->adj_hist);
+  for (int b = 0; b < 2; ++b) {
+    dfree(h->adj_a[b]);
+    dfree(h->adj_w[b]);
+  }
+  dfree(h->adj_state); dfree(h->adj_p); dfree(h->adj_h); dfree(h->adj_rho); dfree(h->adj_g);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -546,6 +574,34 @@ __global__ void __launch_bounds__(ERR_TPB) k_error(const double* ux, const doubl
     part[2 * blockIdx.x] = s1[0];
     part[2 * blockIdx.x + 1] = s2[0];
   }
+}
+
+// One time step on the handle's stream: particle kernel, then the step
+// kernel (the body of lbm_step's loop).
+int enqueue_step(lbm_sim* h) {
+  const int every = h->p.series_every;
+  if (h->series && every > 0 && (h->kk + 1) / every - h->drained_kk / every > h->series_cap) {
+    int rc = drain_series(h);
+    if (rc) return rc;
+  }
+  if (h->prof) {
+    if (h->ev_used + 3 > 3 * 65536) {
+      int rc = profile_flush(h);
+      if (rc) return rc;
+    }
+    CK(record_event(h));
+  }
+  ParticleArgs pa = particle_args(h);
+  CK(launch_particles(pa, h->stream));
+  if (h->prof) CK(record_event(h));
+  h->kk += 1;
+  LatticeArgs a = lattice_args(h);
+  CK(launch_lattice(h, a, 0));
+  if (h->prof) CK(record_event(h));
+  h->cur ^= 1;
+  h->prev_post_bc = false;
+  h->partials_valid = true;
+  return LBM_OK;
 }
 
 }  // namespace
@@ -835,29 +891,9 @@ int lbm_step(lbm_sim* h, int32_t nsteps) {
   int st = sticky_status(h);
   if (st) return st;
   cudaSetDevice(h->p.device);
-  const int every = h->p.series_every;
   for (int32_t s = 0; s < nsteps; ++s) {
-    if (h->series && every > 0 && (h->kk + 1) / every - h->drained_kk / every > h->series_cap) {
-      int rc = drain_series(h);
-      if (rc) return rc;
-    }
-    if (h->prof) {
-      if (h->ev_used + 3 > 3 * 65536) {
-        int rc = profile_flush(h);
-        if (rc) return rc;
-      }
-      CK(record_event(h));
-    }
-    ParticleArgs pa = particle_args(h);
-    CK(launch_particles(pa, h->stream));
-    if (h->prof) CK(record_event(h));
-    h->kk += 1;
-    LatticeArgs a = lattice_args(h);
-    CK(launch_lattice(h, a, 0));
-    if (h->prof) CK(record_event(h));
-    h->cur ^= 1;
-    h->prev_post_bc = false;
-    h->partials_valid = true;
+    int rc = enqueue_step(h);
+    if (rc) return rc;
   }
   h->out_kk = -1;
   CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1149,3 +1185,304 @@ const char* lbm_strerror(int code) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Adjoint sweep.  Forward: the time loop from step 0 to n1, keeping every
+// step's particle records and, every L steps, a checkpoint of the state
+// after that step (f*, omega, records, FORCE sums, D_PW).  Reverse, segment
+// by segment from the last: restore the checkpoint into slot 0, recompute
+// the segment forward with the step kernel writing each f*(n), omega(n) into
+// its own slot, then run the level kernels from the segment's last level to
+// its first, each followed by the particle kernel of the step before.
+namespace {
+
+size_t adj_slot_bytes(const lbm_sim* h) { return (size_t)10 * h->g.plane * h->esz; }
+size_t adj_ckp_len(const lbm_sim* h) { return (size_t)(PS + 6) * h->npad + 1; }
+
+int adj_reserve(lbm_sim* h, int nslots, int nck, long long nhist) {
+  int rc;
+  const size_t sb = adj_slot_bytes(h);
+  if (nslots > h->adj_nslots) {
+    dfree(h->adj_slots);
+    h->adj_nslots = 0;
+    if ((rc = dalloc(&h->adj_slots, sb * nslots))) return rc;
+    h->adj_tm.assign(nslots, CUtensorMap{});
+    for (int s = 0; s < nslots; ++s)
+      if ((rc = encode_f_map(h, h->adj_slots + sb * s, &h->adj_tm[s]))) return rc;
+    h->adj_nslots = nslots;
+  }
+  if (nck > h->adj_nck || h->adj_npad != h->npad) {
+    dfree(h->adj_ck);
+    dfree(h->adj_ckp);
+    h->adj_nck = 0;
+    if (nck > 0 && (rc = dalloc(&h->adj_ck, sb * nck))) return rc;
+    if ((rc = dalloc(&h->adj_ckp, adj_ckp_len(h) * (nck + 1)))) return rc;
+    h->adj_nck = nck;
+  }
+  if (nhist > h->adj_nhist || h->adj_npad != h->npad) {
+    dfree(h->adj_hist);
+    h->adj_nhist = 0;
+    if ((rc = dalloc(&h->adj_hist, (size_t)nhist * PS * h->npad))) return rc;
+    h->adj_nhist = nhist;
+  }
+  if (!h->adj_a[0]) {
+    for (int b = 0; b < 2; ++b) {
+      if ((rc = dalloc(reinterpret_cast<unsigned char**>(&h->adj_a[b]), 9 * h->g.plane * h->esz)))
+        return rc;
+      if ((rc = dalloc(reinterpret_cast<unsigned char**>(&h->adj_w[b]), h->g.plane * h->esz)))
+        return rc;
+    }
+    if ((rc = dalloc(&h->adj_g, (size_t)2 * h->g.nbx * h->g.nby))) return rc;
+  }
+  if (h->adj_npad != h->npad) {
+    dfree(h->adj_state); dfree(h->adj_p); dfree(h->adj_h); dfree(h->adj_rho);
+    const size_t np = (size_t)h->npad;
+    if ((rc = dalloc(&h->adj_state, 8 * np)) || (rc = dalloc(&h->adj_p, 5 * np)) ||
+        (rc = dalloc(&h->adj_h, 3 * np)) || (rc = dalloc(&h->adj_rho, np)))
+      return rc;
+    h->adj_npad = h->npad;
+  }
+  return LBM_OK;
+}
+
+// Small state (records, FORCE sums, D_PW) into / out of checkpoint entry c.
+cudaError_t adj_save_small(lbm_sim* h, int c) {
+  double* d = h->adj_ckp + adj_ckp_len(h) * c;
+  const size_t np = (size_t)h->npad;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(d, h->ps, PS * np * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(d + PS * np, h->facc, 6 * np * sizeof(double),
+                           cudaMemcpyDeviceToDevice, h->stream)) != cudaSuccess)
+    return e;
+  return cudaMemcpyAsync(d + (PS + 6) * np, h->stale_dpw, sizeof(double),
+                         cudaMemcpyDeviceToDevice, h->stream);
+}
+
+int adj_load_small(lbm_sim* h, int c, long long kk, bool partials) {
+  const double* d = h->adj_ckp + adj_ckp_len(h) * c;
+  const size_t np = (size_t)h->npad;
+  CK(cudaMemcpyAsync(h->ps, d, PS * np * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->facc, d + PS * np, 6 * np * sizeof(double), cudaMemcpyDeviceToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->stale_dpw, d + (PS + 6) * np, sizeof(double), cudaMemcpyDeviceToDevice,
+                     h->stream));
+  h->kk = kk;
+  CK(cudaMemcpyAsync(h->d_kk, &h->kk, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));  // &h->kk is pageable
+  h->partials_valid = partials;
+  return launch_tiles(h);
+}
+
+// f* and omega of the current state (f[cur], om[cur]) into a 10-plane block.
+cudaError_t adj_save_fields(lbm_sim* h, unsigned char* dst) {
+  const size_t pb = (size_t)h->g.plane * h->esz;
+  cudaError_t e = cudaMemcpyAsync(dst, h->f[h->cur], 9 * pb, cudaMemcpyDeviceToDevice, h->stream);
+  if (e != cudaSuccess || !h->m.bingham) return e;
+  return cudaMemcpyAsync(dst + 9 * pb, h->om[h->cur], pb, cudaMemcpyDeviceToDevice, h->stream);
+}
+
+// One forward step reading slot s and writing slot s + 1.
+int adj_step_slots(lbm_sim* h, int s) {
+  const size_t sb = adj_slot_bytes(h), pb = (size_t)h->g.plane * h->esz;
+  unsigned char* src = h->adj_slots + sb * s;
+  unsigned char* dst = src + sb;
+  ParticleArgs pa = particle_args(h);
+  CK(launch_particles(pa, h->stream));
+  h->kk += 1;
+  LatticeArgs a = lattice_args(h);
+  a.src = src;
+  a.dst = dst;
+  a.om_src = src + 9 * pb;
+  a.om_dst = dst + 9 * pb;
+  if (h->prec == LBM_FP64) CK(launch_step_fp64(a, &h->adj_tm[s], h->stream));
+  else CK(launch_step_fp32(a, &h->adj_tm[s], h->stream));
+  h->partials_valid = true;
+  return LBM_OK;
+}
+
+AdjParticleArgs adj_particle_args(lbm_sim* h, const lbm_objective* obj, long long n) {
+  AdjParticleArgs q{};
+  const size_t rec = (size_t)PS * h->npad;
+  q.prev = h->adj_hist + rec * (n - 1);
+  q.cur = h->adj_hist + rec * n;
+  q.a_state = h->adj_state;
+  q.a_p = h->adj_p;
+  q.a_h = h->adj_h;
+  q.a_rho = h->adj_rho;
+  q.np = h->np;
+  q.npad = h->npad;
+  q.n = n;
+  q.n0 = obj->n0;
+  q.n1 = obj->n1;
+  q.obj_p = obj->particle;
+  q.obj_c = obj->component;
+  q.obj_w = 1.0 / (double)(obj->n1 - obj->n0 + 1);
+  q.wall_model = h->p.wall_model;
+  q.rep_zeta = h->p.rep_zeta;
+  q.eps_p = h->p.eps_p;
+  q.eps_w = h->p.eps_w;
+  q.e_p = h->p.e_p;
+  q.e_w = h->p.e_w;
+  q.c_ij = h->p.c_ij;
+  q.mirror_top = h->p.wall_mirror_top;
+  q.mirror_left = h->p.wall_mirror_left;
+  q.rho0 = h->p.rho0;
+  q.gravity = h->p.gravity;
+  q.nx = h->p.nx;
+  q.ny = h->p.ny;
+  return q;
+}
+
+cudaError_t adj_level(lbm_sim* h, long long n, const unsigned char* slot, const void* a_in,
+                      const void* aw_in, void* a_out, void* aw_out) {
+  AdjLatticeArgs a{};
+  a.g = h->g;
+  a.m = h->m;
+  const size_t pb = (size_t)h->g.plane * h->esz;
+  a.fs = slot;
+  a.oms = slot ? slot + 9 * pb : nullptr;
+  a.a_in = a_in;
+  a.aw_in = aw_in;
+  a.a_out = a_out;
+  a.aw_out = aw_out;
+  a.ps = h->adj_hist + (size_t)PS * h->npad * n;
+  a.a_h = h->adj_h;
+  a.a_p = h->adj_p;
+  a.gacc = h->adj_g;
+  a.np = h->np;
+  a.npad = h->npad;
+  a.level0 = n == 0 ? 1 : 0;
+  a.kappa = 36.0 * h->p.d_mrt;
+  return h->prec == LBM_FP64 ? launch_adj_lattice_fp64(a, h->stream)
+                             : launch_adj_lattice_fp32(a, h->stream);
+}
+
+}  // namespace
+
+extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, double* grads) {
+  if (!h || !obj || !grads || obj->struct_size != (int32_t)sizeof(lbm_objective))
+    return LBM_E_INVALID;
+  const lbm_params& p = h->p;
+  if (h->kk != 0 || h->np < 1 || h->np > ADJ_MAX_PARTICLES) return LBM_E_INVALID;
+  if (obj->particle < 0 || obj->particle >= h->np || obj->n0 < 1 || obj->n1 < obj->n0 ||
+      obj->checkpoint_every < 0)
+    return LBM_E_INVALID;
+  const int comp = obj->component;
+  if (comp != LBM_OBJ_X && comp != LBM_OBJ_Y && comp != LBM_OBJ_U && comp != LBM_OBJ_V &&
+      comp != LBM_OBJ_W)
+    return LBM_E_INVALID;
+  if ((p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB) ||
+      (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM) ||
+      p.strain_model != LBM_STRAIN_MEQ || p.motion != LBM_MOTION_FREE ||
+      (h->np > 1 && p.contact_test != LBM_CONTACT_DPP))
+    return LBM_E_INVALID;
+  int st = sticky_status(h);
+  if (st) return st;
+  cudaSetDevice(p.device);
+  const long long N = obj->n1;
+  const long long nlev = N - 1;  // lattice levels 1..N-1 act on the objective
+  long long L = obj->checkpoint_every > 0 ? obj->checkpoint_every
+                                          : std::max<long long>(1, std::llround(std::sqrt((double)N)));
+  L = std::max<long long>(1, std::min<long long>(L, std::max<long long>(nlev, 1)));
+  const int C = nlev > 0 ? (int)((nlev + L - 1) / L) : 0;
+  int rc = adj_reserve(h, (int)L, C, N + 1);
+  if (rc) return rc;
+  const size_t rec = (size_t)PS * h->npad;
+  const size_t sb = adj_slot_bytes(h);
+
+  // ---- forward --------------------------------------------------------------
+  CK(cudaMemcpyAsync(h->adj_hist, h->ps, rec * sizeof(double), cudaMemcpyDeviceToDevice,
+                     h->stream));
+  std::vector<char> ck_partials(C + 1, 0);
+  for (long long n = 1; n <= N; ++n) {
+    if ((n - 1) % L == 0 && (n - 1) / L < C) {
+      const int c = (int)((n - 1) / L);
+      CK(adj_save_fields(h, h->adj_ck + sb * c));
+      CK(adj_save_small(h, c));
+      ck_partials[c] = h->partials_valid ? 1 : 0;
+    }
+    if ((rc = enqueue_step(h))) return rc;
+    CK(cudaMemcpyAsync(h->adj_hist + rec * n, h->ps, rec * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->stream));
+  }
+  h->out_kk = -1;
+  CK(adj_save_small(h, C));  // state after step N, put back at the end
+  const bool final_partials = h->partials_valid;
+
+  // ---- reverse --------------------------------------------------------------
+  const size_t np = (size_t)h->npad;
+  CK(cudaMemsetAsync(h->adj_state, 0, 8 * np * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(h->adj_p, 0, 5 * np * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(h->adj_h, 0, 3 * np * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(h->adj_rho, 0, np * sizeof(double), h->stream));
+  CK(cudaMemsetAsync(h->adj_g, 0, 2 * (size_t)h->g.nbx * h->g.nby * sizeof(double), h->stream));
+  struct Restore {  // recomputed steps record no history and no profile
+    lbm_sim* h;
+    int every;
+    bool prof;
+    ~Restore() {
+      h->p.series_every = every;
+      h->prof = prof;
+    }
+  } restore{h, h->p.series_every, h->prof};
+  h->p.series_every = 0;
+  h->prof = false;
+  CK(launch_adj_particles(adj_particle_args(h, obj, N), h->stream));
+  int ain = 0;
+  bool have = false;
+  for (int c = C - 1; c >= 0 && rc == LBM_OK; --c) {
+    const long long t0 = (long long)c * L;
+    const long long hi = std::min<long long>(t0 + L, nlev);
+    CK(cudaMemcpyAsync(h->adj_slots, h->adj_ck + sb * c, sb, cudaMemcpyDeviceToDevice, h->stream));
+    if ((rc = adj_load_small(h, c, t0, ck_partials[c] != 0))) break;
+    for (int s = 0; t0 + 1 + s < hi; ++s)
+      if ((rc = adj_step_slots(h, s))) break;
+    if (rc) break;
+    for (long long n = hi; n >= t0 + 1; --n) {
+      const unsigned char* slot = h->adj_slots + sb * (size_t)(n - t0 - 1);
+      CK(adj_level(h, n, slot, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
+                   h->adj_a[ain ^ 1], h->adj_w[ain ^ 1]));
+      have = true;
+      ain ^= 1;
+      CK(launch_adj_particles(adj_particle_args(h, obj, n), h->stream));
+    }
+  }
+  if (rc) return rc;
+  // level 0: the collision of step 1 from INITIALIZE's state (nu, tau_y only)
+  CK(adj_level(h, 0, nullptr, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
+               nullptr, nullptr));
+  // the handle back at step N
+  if ((rc = adj_load_small(h, C, N, final_partials))) return rc;
+
+  // ---- results ----------------------------------------------------------------
+  std::vector<double> sv(8 * np), rv(np), gv(2 * (size_t)h->g.nbx * h->g.nby);
+  CK(d2h(h, sv.data(), h->adj_state, sv.size() * sizeof(double)));
+  CK(d2h(h, rv.data(), h->adj_rho, rv.size() * sizeof(double)));
+  CK(d2h(h, gv.data(), h->adj_g, gv.size() * sizeof(double)));
+  std::vector<double> hist((size_t)(N + 1) * rec);
+  CK(d2h(h, hist.data(), h->adj_hist, hist.size() * sizeof(double)));
+  CK(cudaStreamSynchronize(h->stream));
+  double gnu = 0.0, gty = 0.0;
+  for (size_t b = 0; b < gv.size(); b += 2) {
+    gnu += gv[b];
+    gty += gv[b + 1];
+  }
+  grads[LBM_GRAD_TAU_Y] = gty;
+  grads[LBM_GRAD_NU] = gnu;
+  for (int q = 0; q < h->np; ++q) {
+    grads[LBM_GRAD_HEAD + LBM_GRAD_PER * q + 0] = rv[q];
+    grads[LBM_GRAD_HEAD + LBM_GRAD_PER * q + 1] = sv[q];
+    grads[LBM_GRAD_HEAD + LBM_GRAD_PER * q + 2] = sv[np + q];
+  }
+  if (value) {
+    const int field = comp == LBM_OBJ_X ? P_X : comp == LBM_OBJ_Y ? P_Y : comp == LBM_OBJ_U ? P_U
+                    : comp == LBM_OBJ_V ? P_V : P_W;
+    double s = 0.0;
+    for (long long n = obj->n0; n <= obj->n1; ++n)
+      s += hist[rec * n + (size_t)field * np + obj->particle];
+    *value = s / (double)(obj->n1 - obj->n0 + 1);
+  }
+  return refreshed_status(h);
+}

@@ -202,6 +202,54 @@ cudaError_t launch_tile_order(const ParticleArgs& a, int buf, cudaStream_t s);
 // set_particles / set_state.
 cudaError_t launch_tiles_only(const ParticleArgs& a, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Adjoint (reverse-mode) sweep, lbm_adjoint.cu.  Level n of the forward is
+// the step kernel that reads f*(n), omega(n) and the particle records of
+// step n and produces FORCE(n), f*(n+1), omega(n+1); the particle kernel of
+// step n+1 then maps (records n, FORCE(n)) to records n+1.
+constexpr int ADJ_MAX_PARTICLES = 64;
+
+// Adjoint field of the populations: a[k] is dJ/dF(k) of the populations
+// after streaming and boundary conditions, stored like f (plane_of(k) planes).
+struct AdjLatticeArgs {
+  Geometry g;
+  Model m;
+  const void* fs;       // f*(n) (T planes); unused at level 0
+  const void* oms;      // omega(n) (T), Bingham
+  const void* a_in;     // dJ/dF(n+1) (T planes), null: zero
+  const void* aw_in;    // dJ/domega(n+1) (T), null: zero
+  void* a_out;          // dJ/dF(n) (T planes); unused at level 0
+  void* aw_out;         // dJ/domega(n) (T), Bingham
+  const double* ps;     // particle records of step n, [PS][npad]
+  const double* a_h;    // dJ/dFORCE(n), [3][npad] (x, y, torque)
+  double* a_p;          // += lattice part of dJ/d(records n): [5][npad] x y u v w
+  double* gacc;         // [blocks][2] += (dJ/dnu, dJ/dtau_y), one slot per block
+  int np, npad;
+  int level0;           // 1: the collision of step 1 from INITIALIZE's state
+  double kappa;         // 36*d_mrt: the scale of the collision's inverse transform
+};
+
+struct AdjParticleArgs {
+  const double* prev;   // records of step n-1
+  const double* cur;    // records of step n
+  double* a_state;      // [8][npad] dJ/d(state): x y u v w uo vo wo, n -> n-1 in place
+  double* a_p;          // [5][npad] lattice part at step n, zeroed here
+  double* a_h;          // [3][npad] out: dJ/dFORCE(n-1)
+  double* a_rho;        // [npad] += dJ/drho_p
+  int np, npad;
+  long long n, n0, n1;  // reverse of the particle update of step n; objective window
+  int obj_p, obj_c;     // observed disk and record field (P_X, P_Y, P_U, P_V, P_W)
+  double obj_w;         // 1 / (n1 - n0 + 1)
+  int wall_model;
+  double rep_zeta, eps_p, eps_w, e_p, e_w, c_ij, mirror_top, mirror_left;
+  double rho0, gravity;
+  int nx, ny;
+};
+
+cudaError_t launch_adj_lattice_fp32(const AdjLatticeArgs& a, cudaStream_t s);
+cudaError_t launch_adj_lattice_fp64(const AdjLatticeArgs& a, cudaStream_t s);
+cudaError_t launch_adj_particles(const AdjParticleArgs& a, cudaStream_t s);
+
 // Host and device decode the force accumulators the same way.
 __host__ __device__ inline double decode_force(unsigned long long hi, unsigned long long lo) {
   return (double)(long long)hi * FDEC_HI + (double)(long long)lo * FDEC_LO;

@@ -423,13 +423,14 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
       if (gam < m.gamma_min_f) {
         nua = sqrtf(NU) + sqrtf(m.m_pap_f * ty);
       } else {
-        nua = sqrtf(NU) + sqrtf(ty / gam) * (1.0f - expf(-sqrtf(m.m_pap_f * gam)));
+        nua = sqrtf(NU) + sqrtf(ty / gam) * -expm1f(-sqrtf(m.m_pap_f * gam));
         nua = nua * nua;
       }
     } else if (gam < m.gamma_min_f) {
       nua = NU + m.m_pap_f * ty;
     } else {
-      nua = NU + (ty / gam) * (1.0f - expf(-(m.m_pap_f * gam)));
+      // 1 - e^(-m gamma) by expm1f: no cancellation where m gamma is small
+      nua = NU + (ty / gam) * -expm1f(-(m.m_pap_f * gam));
     }
     const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
     no.t11 = t11;

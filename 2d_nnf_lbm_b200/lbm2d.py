@@ -44,6 +44,9 @@ LBM_WALL_MIRROR, LBM_WALL_OFFSET, LBM_WALL_NONE = 0, 1, 2
 LBM_CONTACT_DPP, LBM_CONTACT_STALE_DPW = 0, 1
 LBM_PIN, LBM_POUT, LBM_STATE_PER = 8, 16, 20
 LBM_SERIES_HEAD, LBM_SERIES_PER = 2, 12
+LBM_OBJ_X, LBM_OBJ_Y, LBM_OBJ_U, LBM_OBJ_V, LBM_OBJ_W = 0, 1, 3, 4, 5
+LBM_GRAD_TAU_Y, LBM_GRAD_NU, LBM_GRAD_HEAD, LBM_GRAD_PER = 0, 1, 2, 3
+LBM_ADJ_MAX_PARTICLES = 64
 FIELDS = {
     "ux": 0, "uy": 1, "rho": 2, "phi": 3, "gx": 4, "gy": 5,
     "tau11": 6, "tau22": 7, "tau12": 8, "omega": 9,
@@ -201,6 +204,19 @@ def mirror_edges(p: LbmParams) -> None:
     p.wall_mirror_left = 2.0 * edge4
 
 
+class LbmObjective(ctypes.Structure):
+    """lbm_objective: J = mean of record field `component` of disk `particle`
+    over steps n0..n1."""
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("particle", ctypes.c_int32),
+        ("component", ctypes.c_int32),
+        ("checkpoint_every", ctypes.c_int32),
+        ("n0", ctypes.c_int64),
+        ("n1", ctypes.c_int64),
+    ]
+
+
 class LbmError(RuntimeError):
     def __init__(self, code: int, where: str, detail: str = ""):
         self.code = code
@@ -253,6 +269,7 @@ def load_library():
         "lbm_profile_read": ([vp, dp, P(ctypes.c_int64)], ctypes.c_int),
         "lbm_strerror": ([ctypes.c_int], ctypes.c_char_p),
         "lbm_fields_noalloc": ([P(LbmParams), vp, ctypes.c_int32, vp, vp, vp], ctypes.c_int),
+        "lbm_adjoint": ([vp, P(LbmObjective), dp, dp], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -399,3 +416,18 @@ class Simulation:
         n = (ctypes.c_int64 * 2)()
         self._check(self.lib.lbm_profile_read(self._h, ms, n), "lbm_profile_read")
         return (ms[0], ms[1]), (n[0], n[1])
+
+    def adjoint(self, n0: int, n1: int, particle: int = 0, component: int = LBM_OBJ_V,
+                checkpoint_every: int = 0):
+        """lbm_adjoint from step 0: J = mean of `component` of disk `particle`
+        over steps n0..n1 and its gradient, a dict with tau_y, nu and per-disk
+        arrays rho_p, x0, y0.  The simulation is left at step n1."""
+        obj = LbmObjective(ctypes.sizeof(LbmObjective), particle, component, checkpoint_every,
+                           n0, n1)
+        g = np.zeros(LBM_GRAD_HEAD + LBM_GRAD_PER * max(self.np, 1))
+        v = ctypes.c_double()
+        self._check(self.lib.lbm_adjoint(self._h, ctypes.byref(obj), ctypes.byref(v), _dptr(g)),
+                    "lbm_adjoint")
+        per = g[LBM_GRAD_HEAD:LBM_GRAD_HEAD + LBM_GRAD_PER * self.np].reshape(-1, LBM_GRAD_PER)
+        return v.value, {"tau_y": g[LBM_GRAD_TAU_Y], "nu": g[LBM_GRAD_NU],
+                         "rho_p": per[:, 0].copy(), "x0": per[:, 1].copy(), "y0": per[:, 2].copy()}

@@ -249,6 +249,37 @@ int lbm_profile_read(lbm_sim* h, double* ms, int64_t* launches);
 
 const char* lbm_strerror(int code);
 
+/* Adjoint gradients of a particle observable (no counterpart in the
+ * reference, which has no derivatives).  The objective is the mean of one
+ * field of disk `particle` over steps n0..n1 (the record after each step's
+ * Newton-Euler update, C1:247-259):
+ *   J = sum_{n=n0..n1} state_n[component] / (n1 - n0 + 1).
+ * lbm_adjoint runs the forward time loop from step 0 to n1 -- the handle
+ * must be at step 0 with its disks set, and is left at step n1 as lbm_step
+ * would leave it, history records included -- then the reverse sweep:
+ * checkpoints every `checkpoint_every` steps (0: round(sqrt(n1))), each
+ * segment recomputed forward and its states reversed through the transposed
+ * collision / streaming / boundary / SPM / force / Newton-Euler steps.
+ * grads receives 2 + 3*np doubles:
+ *   [LBM_GRAD_TAU_Y] dJ/dtau_y   [LBM_GRAD_NU] dJ/dnu (plastic viscosity)
+ *   then per disk p: dJ/drho_p, dJ/dx0, dJ/dy0 at LBM_GRAD_HEAD + 3p.
+ * Supported: Newtonian or Bingham (Papanastasiou, m_neq strain rate), Zou-He
+ * or half-way bounce-back walls, free motion, at most LBM_ADJ_MAX_PARTICLES
+ * disks, with the pair-distance contact test when np > 1; anything else
+ * returns LBM_E_INVALID before any work.  The repulsion constants (c_ij)
+ * are held fixed. */
+#define LBM_ADJ_MAX_PARTICLES 64
+enum { LBM_OBJ_X = 0, LBM_OBJ_Y = 1, LBM_OBJ_U = 3, LBM_OBJ_V = 4, LBM_OBJ_W = 5 };
+enum { LBM_GRAD_TAU_Y = 0, LBM_GRAD_NU = 1, LBM_GRAD_HEAD = 2, LBM_GRAD_PER = 3 };
+typedef struct lbm_objective {
+    int32_t struct_size;      /* sizeof(lbm_objective) */
+    int32_t particle;         /* observed disk, 0..np-1 */
+    int32_t component;        /* LBM_OBJ_* */
+    int32_t checkpoint_every; /* steps between checkpoints; 0: round(sqrt(n1)) */
+    int64_t n0, n1;           /* window, 1 <= n0 <= n1 */
+} lbm_objective;
+int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, double* grads);
+
 /* Output fields of a state held in caller-owned device memory, computed
  * without allocating anything (no counterpart in the reference).
  *
