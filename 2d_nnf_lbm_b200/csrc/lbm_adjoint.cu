@@ -182,30 +182,41 @@ __device__ __forceinline__ double tcos(double x) { return cos(x); }
 __device__ __forceinline__ float texpm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double texpm1(double x) { return expm1(x); }
 
-// g1 = (1 - e^-x)/x and r = (1 - e^-x - x e^-x)/x^2 for x >= 0, free of
-// cancellation: the Taylor series of e^-x below x = 0.1 (terms to x^12),
-// expm1 above.  The Papanastasiou viscosity is nu + tau_y m g1(m gamma) and
-// its derivative in gamma is -tau_y m^2 r(m gamma).
+// Taylor coefficients: g1 = (1 - e^-x)/x = sum_k (-1)^(k+1) x^(k-1)/k! and
+// r = (1 - e^-x - x e^-x)/x^2 = sum_k (-1)^k (k-1) x^(k-2)/k!; 1/k! below.
+#define LBM_IF(k) (1.0 / (k))
+__device__ __forceinline__ double inv_fact(int k) {
+  constexpr double F[15] = {1.0, 1.0, LBM_IF(2.0), LBM_IF(6.0), LBM_IF(24.0), LBM_IF(120.0),
+                            LBM_IF(720.0), LBM_IF(5040.0), LBM_IF(40320.0), LBM_IF(362880.0),
+                            LBM_IF(3628800.0), LBM_IF(39916800.0), LBM_IF(479001600.0),
+                            LBM_IF(6227020800.0), LBM_IF(87178291200.0)};
+  return F[k];
+}
+#undef LBM_IF
+__device__ __forceinline__ double g1_coef(int k) { return (k % 2 ? 1.0 : -1.0) * inv_fact(k); }
+__device__ __forceinline__ double r_coef(int k) { return (k % 2 ? -1.0 : 1.0) * (k - 1) * inv_fact(k); }
+
+// g1 and r for x >= 0 without cancellation: the series below x = 0.1 (terms
+// to x^7 in FP32, x^13 in FP64; the first omitted term is below the type's
+// rounding), expm1 above.  The Papanastasiou viscosity is
+// nu + tau_y m g1(m gamma) and its derivative in gamma -tau_y m^2 r(m gamma).
 template <class T>
 __device__ __forceinline__ void papanastasiou_terms(T x, T* g1, T* r) {
+  constexpr int K = sizeof(T) == 8 ? 14 : 8;
   if (x < (T)0.1) {
-    T t = (T)1, u = (T)0.5, sg = (T)1, sr = (T)0.5;
-    t = -x * (T)0.5;
-    sg += t;
+    T sg = (T)g1_coef(K), sr = (T)r_coef(K);
 #pragma unroll
-    for (int k = 3; k <= 14; ++k) {
-      t = t * -x / (T)k;
-      sg += t;
-      u = u * -x / (T)k;
-      sr += (T)(k - 1) * u;
-    }
+    for (int k = K - 1; k >= 1; --k) sg = sg * x + (T)g1_coef(k);
+#pragma unroll
+    for (int k = K - 1; k >= 2; --k) sr = sr * x + (T)r_coef(k);
     *g1 = sg;
     *r = sr;
     return;
   }
+  const T ix = (T)1 / x;
   const T em = -texpm1(-x);
-  *g1 = em / x;
-  *r = (em - x * texp(-x)) / (x * x);
+  *g1 = em * ix;
+  *r = (em - x * texp(-x)) * ix * ix;
 }
 
 template <class T>
@@ -230,8 +241,11 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   __shared__ double s_g[ADJ_TPB / 32][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i = blockIdx.x * TX + (tid % TX), j = blockIdx.y * TY + (tid / TX);
+  // the next particle adjoint kernel may launch; it waits for this grid
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
-  // disks whose support reaches this block, in index order
+  // disks whose support reaches this block, in index order (records of step
+  // n, written by the forward pass)
   if (tid == 0) {
     int c = 0;
     if (!a.level0) {
@@ -248,9 +262,6 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
         s_u[c] = P[P_U];
         s_v[c] = P[P_V];
         s_w[c] = P[P_W];
-        s_ax[c] = a.a_h[p];
-        s_ay[c] = a.a_h[a.npad + p];
-        s_at[c] = a.a_h[2 * a.npad + p];
         ++c;
       }
     }
@@ -311,9 +322,10 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   }
   const T ux = upx + (T)0.5 * Gx, uy = upy + (T)0.5 * Gy;
   const bool node_omega = m.bingham && !a.level0;
-  const double om = node_omega && act ? (double)static_cast<const T*>(a.oms)[n] : m.omega;
-  const T sw = (T)om;
-  const T sq = m.q_of_omega ? (T)(8. * (2. - om) / (8. - om)) : (T)m.s_q;
+  const T om = node_omega && act ? static_cast<const T*>(a.oms)[n] : (T)m.omega;
+  const T sw = om;
+  const T i8w = (T)1 / ((T)8 - om);
+  const T sq = m.q_of_omega ? (T)8 * ((T)2 - om) * i8w : (T)m.s_q;
   const T s1 = (T)m.s_e, s2 = (T)m.s_eps;
   const T kap = (T)a.kappa;
   const T U2 = ux * ux + uy * uy;
@@ -336,15 +348,18 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   // f*(n+1) = kappa M^-1 m' + const  ->  dJ/dm' = kappa D^-1 M dJ/df*
   T am[9];
   moments9<T>(ahs, am);
-  am[0] *= kap / (T)9;
-  am[1] *= kap / (T)36;
-  am[2] *= kap / (T)36;
-  am[3] *= kap / (T)6;
-  am[4] *= kap / (T)12;
-  am[5] *= kap / (T)6;
-  am[6] *= kap / (T)12;
-  am[7] *= kap / (T)4;
-  am[8] *= kap / (T)4;
+  {
+    const T k36 = kap * (T)(1.0 / 36.0);
+    am[0] *= (T)4 * k36;
+    am[1] *= k36;
+    am[2] *= k36;
+    am[3] *= (T)6 * k36;
+    am[4] *= (T)3 * k36;
+    am[5] *= (T)6 * k36;
+    am[6] *= (T)3 * k36;
+    am[7] *= (T)9 * k36;
+    am[8] *= (T)9 * k36;
+  }
   // m' = M - S m_neq + (1 - S/2) m_F
   T aM[9];
 #pragma unroll
@@ -381,9 +396,10 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
     const T agam = low ? (T)0 : -anuA * ty * mp * mp * rq;
     T ad11 = (T)0, ad22 = (T)0, ad12 = (T)0;
     if (gam > (T)0) {
-      ad11 = agam * (T)2 * d11 / gam;
-      ad22 = agam * (T)2 * d22 / gam;
-      ad12 = agam * (T)4 * d12 / gam;
+      const T q = (T)2 * agam / gam;
+      ad11 = q * d11;
+      ad22 = q * d22;
+      ad12 = (T)2 * q * d12;
     }
     arho -= (ad11 * d11 + ad22 * d22 + ad12 * d12) * ir;
     const T aD11 = ad11 * ir, aD22 = ad22 * ir, aD12 = ad12 * ir;
@@ -428,11 +444,11 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   // rates of omega (C6:1002-1021)
   {
     T aom = asw;
-    if (m.q_of_omega) aom += asq * (T)(-48.0 / ((8.0 - om) * (8.0 - om)));
+    if (m.q_of_omega) aom += asq * (T)-48 * i8w * i8w;
     if (node_omega) {
       if (act) static_cast<T*>(a.aw_out)[n] = aom;
     } else if (act) {
-      gnu += (double)aom * (-3.0 * m.omega * m.omega);  // omega = 1/(3 nu + 1/2)
+      gnu += (double)(aom * (T)(-3.0 * m.omega * m.omega));  // omega = 1/(3 nu + 1/2)
     }
   }
   // u = u_pred + G/2 (C1:1138-1152); G = phi (u_p - u_pred) of the winner
@@ -445,6 +461,16 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   }
 
   // ---- disks: G of the winner, FORCE(n), phi and the rigid velocity --------
+  // dJ/dFORCE(n) comes from the particle adjoint kernel launched before this
+  // one, which also clears a_p after reading it: wait for it here.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (tid < nc) {
+    const int p = s_idx[tid];
+    s_ax[tid] = a.a_h[p];
+    s_ay[tid] = a.a_h[a.npad + p];
+    s_at[tid] = a.a_h[2 * a.npad + p];
+  }
+  __syncthreads();
   for (int c = 0; c < nc; ++c) {
     double cx = 0.0, cy = 0.0, cu = 0.0, cv = 0.0, cw = 0.0;
     if (act) {
@@ -483,9 +509,9 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
         const T zh = (T)(0.5 * m.zeta);
         if (Dd > -zh && Dd < zh && r > (T)0) {
           const T k = (T)(m.pi / m.zeta);
-          const T aD = aphi * (T)0.5 * k * tcos(k * Dd);
-          adi -= aD * di / r;
-          adj -= aD * dj / r;
+          const T aD = aphi * (T)0.5 * k * tcos(k * Dd) / r;
+          adi -= aD * di;
+          adj -= aD * dj;
         }
         cx = -(double)adi;
         cy = -(double)adj;
@@ -566,6 +592,10 @@ __device__ __forceinline__ void glowinski(double r, double contact, double zeta,
 __global__ void __launch_bounds__(ADJ_MAX_PARTICLES) k_adj_particles(const AdjParticleArgs a) {
   __shared__ double s_fx[ADJ_MAX_PARTICLES], s_fy[ADJ_MAX_PARTICLES];
   const int p = threadIdx.x;
+  // launched as a programmatic dependent of the lattice adjoint kernel of
+  // the same step: its per-disk sums and dJ/dF must be complete
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const long long st = a.npad;
   double aX = 0, aY = 0, aUp = 0, aVp = 0, aWp = 0, aUO = 0, aVO = 0, aWO = 0;
   double x = 0, y = 0, D = 0, M = 1, I = 1;
@@ -667,21 +697,34 @@ __global__ void __launch_bounds__(ADJ_MAX_PARTICLES) k_adj_particles(const AdjPa
   }
 }
 
-template <class T>
-cudaError_t launch_adj(const AdjLatticeArgs& a, cudaStream_t s) {
-  dim3 grid(a.g.nbx, a.g.nby);
-  k_adj_lattice<T><<<grid, ADJ_TPB, 0, s>>>(a);
-  return cudaGetLastError();
+template <class K, class A>
+cudaError_t launch_pdl(K kernel, dim3 grid, int block, const A& a, cudaStream_t s, int pdl) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
-cudaError_t launch_adj_lattice_fp32(const AdjLatticeArgs& a, cudaStream_t s) {
-  return launch_adj<float>(a, s);
+cudaError_t launch_adj_lattice_fp32(const AdjLatticeArgs& a, cudaStream_t s, int pdl) {
+  return launch_pdl(k_adj_lattice<float>, dim3(a.g.nbx, a.g.nby), ADJ_TPB, a, s, pdl);
 }
-cudaError_t launch_adj_lattice_fp64(const AdjLatticeArgs& a, cudaStream_t s) {
-  return launch_adj<double>(a, s);
+cudaError_t launch_adj_lattice_fp64(const AdjLatticeArgs& a, cudaStream_t s, int pdl) {
+  return launch_pdl(k_adj_lattice<double>, dim3(a.g.nbx, a.g.nby), ADJ_TPB, a, s, pdl);
 }
 cudaError_t launch_adj_particles(const AdjParticleArgs& a, cudaStream_t s) {
-  k_adj_particles<<<1, ADJ_MAX_PARTICLES, 0, s>>>(a);
+  return launch_pdl(k_adj_particles, dim3(1), ADJ_MAX_PARTICLES, a, s, 1);
+}
+
+__global__ void k_set_ll(long long* p, long long v) { *p = v; }
+
+cudaError_t launch_set_ll(long long* p, long long v, cudaStream_t s) {
+  k_set_ll<<<1, 1, 0, s>>>(p, v);
   return cudaGetLastError();
 }
 

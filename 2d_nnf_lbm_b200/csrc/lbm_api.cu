@@ -105,6 +105,7 @@ struct lbm_sim {
   double* adj_rho = nullptr;           // [npad]
   double* adj_g = nullptr;             // [blocks][2]
   int adj_npad = 0;
+  bool adj_record = false;  // the particle kernel writes adj_hist (forward pass)
 };
 
 namespace {
@@ -254,6 +255,8 @@ ParticleArgs particle_args(lbm_sim* h) {
   a.osc_u = h->p.osc_u;
   a.osc_period = h->p.osc_period;
   a.pi = h->p.pi;
+  a.hist = h->adj_record ? h->adj_hist : nullptr;
+  a.hist_n = h->adj_record ? h->adj_nhist : 0;
   return a;
 }
 
@@ -1269,8 +1272,7 @@ int adj_load_small(lbm_sim* h, int c, long long kk, bool partials) {
   CK(cudaMemcpyAsync(h->stale_dpw, d + (PS + 6) * np, sizeof(double), cudaMemcpyDeviceToDevice,
                      h->stream));
   h->kk = kk;
-  CK(cudaMemcpyAsync(h->d_kk, &h->kk, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));  // &h->kk is pageable
+  CK(launch_set_ll(h->d_kk, kk, h->stream));
   h->partials_valid = partials;
   return launch_tiles(h);
 }
@@ -1336,7 +1338,7 @@ AdjParticleArgs adj_particle_args(lbm_sim* h, const lbm_objective* obj, long lon
 }
 
 cudaError_t adj_level(lbm_sim* h, long long n, const unsigned char* slot, const void* a_in,
-                      const void* aw_in, void* a_out, void* aw_out) {
+                      const void* aw_in, void* a_out, void* aw_out, int pdl) {
   AdjLatticeArgs a{};
   a.g = h->g;
   a.m = h->m;
@@ -1355,8 +1357,8 @@ cudaError_t adj_level(lbm_sim* h, long long n, const unsigned char* slot, const 
   a.npad = h->npad;
   a.level0 = n == 0 ? 1 : 0;
   a.kappa = 36.0 * h->p.d_mrt;
-  return h->prec == LBM_FP64 ? launch_adj_lattice_fp64(a, h->stream)
-                             : launch_adj_lattice_fp32(a, h->stream);
+  return h->prec == LBM_FP64 ? launch_adj_lattice_fp64(a, h->stream, pdl)
+                             : launch_adj_lattice_fp32(a, h->stream, pdl);
 }
 
 }  // namespace
@@ -1396,17 +1398,19 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
   CK(cudaMemcpyAsync(h->adj_hist, h->ps, rec * sizeof(double), cudaMemcpyDeviceToDevice,
                      h->stream));
   std::vector<char> ck_partials(C + 1, 0);
-  for (long long n = 1; n <= N; ++n) {
+  h->adj_record = true;  // the particle kernel stores each step's records
+  for (long long n = 1; n <= N && rc == LBM_OK; ++n) {
     if ((n - 1) % L == 0 && (n - 1) / L < C) {
       const int c = (int)((n - 1) / L);
-      CK(adj_save_fields(h, h->adj_ck + sb * c));
-      CK(adj_save_small(h, c));
+      cudaError_t e = adj_save_fields(h, h->adj_ck + sb * c);
+      if (e == cudaSuccess) e = adj_save_small(h, c);
+      if (e != cudaSuccess) rc = cuda_fail(e);
       ck_partials[c] = h->partials_valid ? 1 : 0;
     }
-    if ((rc = enqueue_step(h))) return rc;
-    CK(cudaMemcpyAsync(h->adj_hist + rec * n, h->ps, rec * sizeof(double),
-                       cudaMemcpyDeviceToDevice, h->stream));
+    if (rc == LBM_OK) rc = enqueue_step(h);
   }
+  h->adj_record = false;
+  if (rc) return rc;
   h->out_kk = -1;
   CK(adj_save_small(h, C));  // state after step N, put back at the end
   const bool final_partials = h->partials_valid;
@@ -1442,8 +1446,10 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
     if (rc) break;
     for (long long n = hi; n >= t0 + 1; --n) {
       const unsigned char* slot = h->adj_slots + sb * (size_t)(n - t0 - 1);
+      // the first level after a recompute reads the slot the step kernel
+      // just wrote: no early start there
       CK(adj_level(h, n, slot, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
-                   h->adj_a[ain ^ 1], h->adj_w[ain ^ 1]));
+                   h->adj_a[ain ^ 1], h->adj_w[ain ^ 1], n == hi ? 0 : 1));
       have = true;
       ain ^= 1;
       CK(launch_adj_particles(adj_particle_args(h, obj, n), h->stream));
@@ -1452,7 +1458,7 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
   if (rc) return rc;
   // level 0: the collision of step 1 from INITIALIZE's state (nu, tau_y only)
   CK(adj_level(h, 0, nullptr, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
-               nullptr, nullptr));
+               nullptr, nullptr, 1));
   // the handle back at step N
   if ((rc = adj_load_small(h, C, N, final_partials))) return rc;
 

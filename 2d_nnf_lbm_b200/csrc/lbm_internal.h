@@ -142,6 +142,9 @@ struct ParticleArgs {
   int* status;
   int nx, ny;
   double zeta;               // SPM interface thickness (tile box radius)
+  // adjoint forward pass: record of step k into hist[k][PS][npad] (k < hist_n)
+  double* hist;
+  long long hist_n;
 };
 
 struct LatticeArgs {
@@ -246,9 +249,13 @@ struct AdjParticleArgs {
   int nx, ny;
 };
 
-cudaError_t launch_adj_lattice_fp32(const AdjLatticeArgs& a, cudaStream_t s);
-cudaError_t launch_adj_lattice_fp64(const AdjLatticeArgs& a, cudaStream_t s);
+// pdl: launch as a programmatic dependent of the previous kernel (which must
+// be the particle adjoint kernel: the lattice kernel waits for it only
+// before reading dJ/dFORCE and adding to a_p).
+cudaError_t launch_adj_lattice_fp32(const AdjLatticeArgs& a, cudaStream_t s, int pdl);
+cudaError_t launch_adj_lattice_fp64(const AdjLatticeArgs& a, cudaStream_t s, int pdl);
 cudaError_t launch_adj_particles(const AdjParticleArgs& a, cudaStream_t s);
+cudaError_t launch_set_ll(long long* p, long long v, cudaStream_t s);
 
 // Host and device decode the force accumulators the same way.
 __host__ __device__ inline double decode_force(unsigned long long hi, unsigned long long lo) {

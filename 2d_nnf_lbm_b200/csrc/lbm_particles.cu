@@ -426,6 +426,10 @@ __global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
       r[6] = frx; r[7] = fry; r[8] = frt;
       r[9] = fh0; r[10] = fh1; r[11] = fh2;
     }
+    if (a.hist && kk < a.hist_n) {
+      double* hr = a.hist + kk * (long long)PS * a.npad + p;
+      for (int f = 0; f < PS; ++f) hr[(long long)f * a.npad] = P[f];
+    }
     const double tdx = nx_ - xt, tdy = ny_ - yt;
     if (!(tdx * tdx + tdy * tdy <= 0.25 * SKIN * SKIN)) s_tiles = 1;
   }
