@@ -17,6 +17,11 @@ Arms:
                      its loop structure (the Fortran itself cannot be built
                      in this image), single-threaded as the reference is
 
+Adjoint (N=1): the "adjoint" object times lbm_adjoint on the adjoint
+workload (400x1200, one Bingham disk, 4000 steps, sqrt(N) checkpoints)
+against the forward time loop and checks its FP32 gradient against FP64
+central differences; --no-adjoint skips it.
+
 Multi-GPU: the hot path does not shard (one simulation, one GPU); --gpus N
 runs N independent replicas (weak scaling), timed as the max over ranks.
 """
@@ -50,6 +55,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint/forward time measurement")
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="steps of the FP32-vs-FP64 trajectory comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
@@ -290,6 +297,93 @@ def trajectory_error(pkg, args, device, steps):
     }
 
 
+def adjoint_measure(pkg, torch, device):
+    """The adjoint workload (400x1200 lattice, one disk D=24, Bn=5, 4000
+    steps, J = mean v_y over steps 3000..4000, sqrt(N) = 63 checkpoints):
+    wall time of lbm_adjoint against the forward time loop, both timed with
+    CUDA events on the handle's stream (the adjoint call synchronises
+    internally, so its interval is its wall time), FP32 and FP64; the FP32
+    gradient against the FP64 adjoint and against FP64 central differences
+    (relative step 1e-4) of the GPU forward."""
+    out = {}
+    res = {}
+    for prec in (1, 0):
+        p, pin, info = pkg.cases.workload_cfg5(prec)
+        p.device = device
+        n0, n1 = info["n0"], info["n1"]
+
+        def timed(fn):
+            sim = pkg.Simulation(p)
+            sim.set_particles(pin)
+            ext = torch.cuda.ExternalStream(sim.stream())
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(ext)
+            r = fn(sim)
+            e1.record(ext)
+            e1.synchronize()
+            sim.close()
+            return e0.elapsed_time(e1), r
+
+        timed(lambda s: s.adjoint(n0, n1))  # buffers allocated, code paged in
+        fwd = min(timed(lambda s: s.step(n1))[0] for _ in range(2))
+        adj, (j, g) = min((timed(lambda s: s.adjoint(n0, n1)) for _ in range(2)),
+                          key=lambda t: t[0])
+        res[prec] = (j, g)
+        out["fp32" if prec else "fp64"] = {"fwd_ms": fwd, "adjoint_ms": adj,
+                                           "adjoint_over_fwd": adj / fwd}
+    p64, pin, info = pkg.cases.workload_cfg5(0)
+    p64.device = device
+    n0, n1 = info["n0"], info["n1"]
+
+    def run_j(q, disks):
+        sim = pkg.Simulation(q)
+        sim.set_particles(disks)
+        sim.step(n0 - 1)
+        v = []
+        for _ in range(n0, n1 + 1):
+            sim.step(1)
+            v.append(sim.particles()[0, 4])
+        sim.close()
+        return float(np.mean(v))
+
+    fd = {}
+    for name in ("tau_y", "nu", "rho_p"):
+        base = {"tau_y": p64.tau_y, "nu": p64.nu, "rho_p": float(pin[0, 7])}[name]
+        d = 1e-4 * abs(base)
+        jj = []
+        for sgn in (1.0, -1.0):
+            q = p64.copy()
+            disks = np.array(pin, copy=True)
+            if name == "tau_y":
+                q.tau_y = base + sgn * d
+            elif name == "nu":
+                q.nu = base + sgn * d
+            else:
+                disks[0, 7] = base + sgn * d
+            jj.append(run_j(q, disks))
+        fd[name] = (jj[0] - jj[1]) / (2 * d)
+    j32, g32 = res[1]
+    j64, g64 = res[0]
+    pick = lambda g, k: float(g[k] if k != "rho_p" else g[k][0])  # noqa: E731
+    out.update({
+        "workload": "Bingham settling 400x1200 (481,601 nodes), disk D=24 rho_p=1.5, Bn=5, "
+                    "tau_p=0.9, m=1e5, 4000 steps, J = mean v_y over steps 3000..4000",
+        "checkpoint_every": int(round(n1 ** 0.5)),
+        "J": j32,
+        "grad_fp32": {k: pick(g32, k) for k in fd},
+        "grad_fp64": {k: pick(g64, k) for k in fd},
+        "fd_fp64": fd,
+        "max_rel_err_fp32_vs_fd": max(abs(pick(g32, k) - fd[k]) / abs(fd[k]) for k in fd),
+        "max_rel_err_fp64_vs_fd": max(abs(pick(g64, k) - fd[k]) / abs(fd[k]) for k in fd),
+        "max_rel_err_fp32_vs_fp64_adjoint": max(abs(pick(g32, k) - pick(g64, k)) /
+                                                abs(pick(g64, k)) for k in fd),
+        "tolerance": 1e-3,
+    })
+    return out
+
+
 def cpu_baseline(pkg, args, seconds):
     """The oracle (reference loop structure, one thread) on the same workload,
     timed over a bounded number of whole time steps."""
@@ -424,6 +518,8 @@ def main():
     }
     if args.accuracy_steps > 0:
         line["trajectory_err"] = trajectory_error(pkg, args, device, args.accuracy_steps)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_measure(pkg, torch, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pkg, args, args.cpu_seconds)
     if rank == 0:
