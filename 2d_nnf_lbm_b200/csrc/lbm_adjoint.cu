@@ -288,6 +288,18 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
       for (int k = 0; k < 9; ++k) h[k] = h[k] - (T)(wexact(k) * m.rho0);
     }
   }
+  // every global load of the node is issued here, before the arithmetic:
+  // omega(n), dJ/dF(n+1) of the transposed pull, dJ/domega(n+1)
+  const bool node_omega = m.bingham && !a.level0;
+  const T om = node_omega && act ? static_cast<const T*>(a.oms)[n] : (T)m.omega;
+  T ahs[9];
+  if (a.a_in && act) {
+    adj_gather<T>(static_cast<const T*>(a.a_in), g, m.bc, i, j, ahs);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ahs[k] = (T)0;
+  }
+  const T awo = (m.bingham && a.aw_in && act) ? static_cast<const T*>(a.aw_in)[n] : (T)0;
   T mh[9];
   moments9<T>(h, mh);
   T drho, rho, upx, upy;
@@ -321,8 +333,6 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
     Gy = phw * (usyw - upy);
   }
   const T ux = upx + (T)0.5 * Gx, uy = upy + (T)0.5 * Gy;
-  const bool node_omega = m.bingham && !a.level0;
-  const T om = node_omega && act ? static_cast<const T*>(a.oms)[n] : (T)m.omega;
   const T sw = om;
   const T i8w = (T)1 / ((T)8 - om);
   const T sq = m.q_of_omega ? (T)8 * ((T)2 - om) * i8w : (T)m.s_q;
@@ -334,16 +344,6 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_lattice(const AdjLatticeArgs a)
   const T mne7 = mh[7] - rho * (ux * ux - uy * uy), mne8 = mh[8] - rho * ux * uy;
   const T Fx = rho * Gx, Fy = rho * Gy;
   const T mf4 = -Fx, mf6 = -Fy, mf7 = (T)2 * (Fx * ux - Fy * uy), mf8 = Fy * ux + Fx * uy;
-
-  // ---- adjoint inputs ------------------------------------------------------
-  T ahs[9];
-  if (a.a_in && act) {
-    adj_gather<T>(static_cast<const T*>(a.a_in), g, m.bc, i, j, ahs);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 9; ++k) ahs[k] = (T)0;
-  }
-  const T awo = (m.bingham && a.aw_in && act) ? static_cast<const T*>(a.aw_in)[n] : (T)0;
 
   // f*(n+1) = kappa M^-1 m' + const  ->  dJ/dm' = kappa D^-1 M dJ/df*
   T am[9];
