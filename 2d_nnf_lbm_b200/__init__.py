@@ -10,6 +10,7 @@ or no CUDA device is present, the calls raise.
 """
 
 from .lbm2d import (  # noqa: F401
+    Batch,
     LbmError,
     LbmObjective,
     LbmParams,

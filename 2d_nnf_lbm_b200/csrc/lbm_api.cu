@@ -1492,3 +1492,301 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
   }
   return refreshed_status(h);
 }
+
+// ===========================================================================
+// Batched time steps.  All simulations of a batch advance in lockstep on the
+// batch's stream: per step one launch of k_particles_batch (block b =
+// simulation b) and one of k_lattice_batch (persistent grid over every
+// simulation's tiles).  Steps run from a captured graph of BATCH_GRAPH_STEPS
+// steps once the tile shape and grid are chosen.
+struct lbm_batch {
+  std::vector<lbm_sim*> sims;
+  int device = 0;
+  int prec = 0;
+  int nsm = 148;
+  cudaStream_t stream = nullptr;
+  BatchSim* d_sims = nullptr;
+  ParticleArgs* d_pargs = nullptr;
+  std::vector<BatchSim> h_sims;
+  std::vector<ParticleArgs> h_pargs;
+  long long total = 0;     // work items at the current shape
+  int shape = -1;          // tuned (or fixed) tile shape, -1: not yet
+  int bpsm = 0;            // persistent blocks per SM
+  bool fixed = false;      // set by lbm_batch_set_tuning
+  cudaGraphExec_t exec = nullptr;
+  int graph_shape = -1, graph_bpsm = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+constexpr int BATCH_GRAPH_STEPS = 8;
+constexpr int BATCH_BPSM[3] = {2, 4, 8};
+
+int batch_grid(const lbm_batch* b) {
+  const long long g = (long long)b->bpsm * b->nsm;
+  return (int)std::max<long long>(1, std::min<long long>(g, b->total));
+}
+
+// Per-simulation arguments at tile shape `shape`, uploaded to the device.
+int batch_upload(lbm_batch* b, int shape) {
+  const int n = (int)b->sims.size();
+  const int bx = batch_bx(shape), by = batch_by(shape);
+  long long first = 0;
+  for (int q = 0; q < n; ++q) {
+    lbm_sim* h = b->sims[q];
+    BatchSim& B = b->h_sims[q];
+    B.a = lattice_args(h);
+    for (int k = 0; k < 2; ++k) {
+      B.f[k] = h->f[k];
+      B.om[k] = h->om[k];
+    }
+    B.kk = h->d_kk;
+    B.rec_slot = h->rec_slot;
+    B.par0 = (int)(((long long)h->cur - h->kk) & 1);
+    B.nbx = (h->p.nx + 1 + bx - 1) / bx;
+    B.first = first;
+    first += (long long)B.nbx * ((h->p.ny + 1 + by - 1) / by);
+    b->h_pargs[q] = particle_args(h);
+  }
+  b->total = first;
+  CK(cudaMemcpyAsync(b->d_sims, b->h_sims.data(), n * sizeof(BatchSim), cudaMemcpyHostToDevice,
+                     b->stream));
+  CK(cudaMemcpyAsync(b->d_pargs, b->h_pargs.data(), n * sizeof(ParticleArgs),
+                     cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));  // the host arrays are pageable and reused
+  return LBM_OK;
+}
+
+cudaError_t batch_launch_step(lbm_batch* b) {
+  cudaError_t e = launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream);
+  if (e != cudaSuccess) return e;
+  return b->prec == LBM_FP64
+             ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, b->shape, batch_grid(b),
+                                 b->stream)
+             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, b->shape, batch_grid(b),
+                                 b->stream);
+}
+
+// Host bookkeeping of s completed batch steps.
+void batch_advance(lbm_batch* b, int s) {
+  for (lbm_sim* h : b->sims) {
+    h->kk += s;
+    h->cur ^= (s & 1);
+    h->prev_post_bc = false;
+    h->partials_valid = true;
+    h->out_kk = -1;
+  }
+}
+
+// Steps every simulation can take before its history ring is full.
+long long batch_room(const lbm_batch* b) {
+  long long room = 1LL << 40;
+  for (const lbm_sim* h : b->sims) {
+    const int every = h->p.series_every;
+    if (!h->series || every <= 0) continue;
+    const long long last = (h->series_cap + h->drained_kk / every + 1) * (long long)every - 1;
+    room = std::min(room, last - h->kk);
+  }
+  return room;
+}
+
+int batch_tune(lbm_batch* b, int32_t& left) {
+  // one timed step per (shape, blocks per SM), results independent of both
+  float best = 1e30f;
+  int bs = 0, bb = BATCH_BPSM[0];
+  for (int sh = 0; sh < BATCH_SHAPES && left > 0; ++sh) {
+    int rc = batch_upload(b, sh);
+    if (rc) return rc;
+    b->shape = sh;
+    for (int k = 0; k < 3 && left > 0 && batch_room(b) > 0; ++k) {
+      b->bpsm = BATCH_BPSM[k];
+      CK(launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream));
+      CK(cudaEventRecord(b->ev[0], b->stream));
+      CK(b->prec == LBM_FP64 ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, sh,
+                                                 batch_grid(b), b->stream)
+                             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, sh,
+                                                 batch_grid(b), b->stream));
+      CK(cudaEventRecord(b->ev[1], b->stream));
+      CK(cudaEventSynchronize(b->ev[1]));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+      batch_advance(b, 1);
+      --left;
+      if (ms < best) {
+        best = ms;
+        bs = sh;
+        bb = BATCH_BPSM[k];
+      }
+      // the next launch decodes the force sums this one left
+      for (ParticleArgs& pa : b->h_pargs) pa.decode_force = 1;
+      CK(cudaMemcpyAsync(b->d_pargs, b->h_pargs.data(), b->h_pargs.size() * sizeof(ParticleArgs),
+                         cudaMemcpyHostToDevice, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+    }
+  }
+  b->shape = bs;
+  b->bpsm = bb;
+  return batch_upload(b, bs);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(const lbm_params* params, int32_t nsim, lbm_batch** out) {
+  if (!params || !out || nsim < 1) return LBM_E_INVALID;
+  *out = nullptr;
+  for (int q = 1; q < nsim; ++q)
+    if (params[q].precision != params[0].precision || params[q].device != params[0].device)
+      return LBM_E_INVALID;
+  lbm_batch* b = new (std::nothrow) lbm_batch();
+  if (!b) return LBM_E_NOMEM;
+  auto fail = [&](int rc) {
+    lbm_batch_destroy(b);
+    return rc;
+  };
+  b->device = params[0].device;
+  b->prec = params[0].precision;
+  for (int q = 0; q < nsim; ++q) {
+    lbm_sim* h = nullptr;
+    int rc = lbm_create(&params[q], &h);
+    if (rc) return fail(rc);
+    b->sims.push_back(h);
+  }
+  cudaSetDevice(b->device);
+  if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess)
+    return fail(LBM_E_CUDA);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess ||
+      prepare_particles_batch() != cudaSuccess)
+    return fail(LBM_E_CUDA);
+  int rc;
+  if ((rc = dalloc(&b->d_sims, nsim)) || (rc = dalloc(&b->d_pargs, nsim))) return fail(rc);
+  b->h_sims.resize(nsim);
+  b->h_pargs.resize(nsim);
+  *out = b;
+  return LBM_OK;
+}
+
+lbm_sim* lbm_batch_sim(lbm_batch* b, int32_t i) {
+  if (!b || i < 0 || i >= (int32_t)b->sims.size()) return nullptr;
+  return b->sims[i];
+}
+
+int lbm_batch_tuning(lbm_batch* b, int32_t* tile_x, int32_t* tile_y, int32_t* blocks_per_sm) {
+  if (!b || !tile_x || !tile_y || !blocks_per_sm) return LBM_E_INVALID;
+  *tile_x = b->shape < 0 ? 0 : batch_bx(b->shape);
+  *tile_y = b->shape < 0 ? 0 : batch_by(b->shape);
+  *blocks_per_sm = b->shape < 0 ? 0 : b->bpsm;
+  return LBM_OK;
+}
+
+int lbm_batch_set_tuning(lbm_batch* b, int32_t tile_x, int32_t tile_y, int32_t blocks_per_sm) {
+  if (!b) return LBM_E_INVALID;
+  if (tile_x == 0) {
+    b->fixed = false;
+    b->shape = -1;
+    return LBM_OK;
+  }
+  int sh = -1;
+  for (int q = 0; q < BATCH_SHAPES; ++q)
+    if (batch_bx(q) == tile_x && batch_by(q) == tile_y) sh = q;
+  if (sh < 0 || blocks_per_sm < 1 || blocks_per_sm > 64) return LBM_E_INVALID;
+  b->shape = sh;
+  b->bpsm = blocks_per_sm;
+  b->fixed = true;
+  return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch* b, int32_t nsteps) {
+  if (!b || nsteps < 0) return LBM_E_INVALID;
+  cudaSetDevice(b->device);
+  for (lbm_sim* h : b->sims) {
+    int st = sticky_status(h);
+    if (st) return st;
+    CK(cudaStreamSynchronize(h->stream));  // the handles' own work first
+  }
+  int rc;
+  int32_t left = nsteps;
+  if (left == 0) return LBM_OK;
+  // a simulation whose force sums are not yet valid (fresh, restarted) takes
+  // one step with its own decode flag before the rest can be uniform
+  if (b->shape < 0) {
+    if ((rc = batch_tune(b, left))) return rc;
+  } else {
+    if ((rc = batch_upload(b, b->shape))) return rc;
+  }
+  while (left > 0) {
+    long long room = batch_room(b);
+    if (room <= 0) {
+      CK(cudaStreamSynchronize(b->stream));
+      for (lbm_sim* h : b->sims)
+        if ((rc = drain_series(h))) return rc;
+      continue;
+    }
+    bool uniform = true;
+    for (const ParticleArgs& pa : b->h_pargs) uniform = uniform && pa.decode_force == 1;
+    const long long chunk = std::min<long long>(left, room);
+    if (uniform && chunk >= BATCH_GRAPH_STEPS) {
+      if (!b->exec || b->graph_shape != b->shape || b->graph_bpsm != b->bpsm) {
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int s = 0; s < BATCH_GRAPH_STEPS && e == cudaSuccess; ++s) e = batch_launch_step(b);
+        cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+          if (g) cudaGraphDestroy(g);
+          return LBM_E_CUDA;
+        }
+        e = cudaGraphInstantiate(&b->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e);
+        b->graph_shape = b->shape;
+        b->graph_bpsm = b->bpsm;
+      }
+      const long long reps = chunk / BATCH_GRAPH_STEPS;
+      for (long long r = 0; r < reps; ++r) CK(cudaGraphLaunch(b->exec, b->stream));
+      batch_advance(b, (int)(reps * BATCH_GRAPH_STEPS));
+      left -= (int32_t)(reps * BATCH_GRAPH_STEPS);
+      continue;
+    }
+    CK(batch_launch_step(b));
+    batch_advance(b, 1);
+    --left;
+    if (!uniform) {
+      for (ParticleArgs& pa : b->h_pargs) pa.decode_force = 1;
+      CK(cudaMemcpyAsync(b->d_pargs, b->h_pargs.data(), b->h_pargs.size() * sizeof(ParticleArgs),
+                         cudaMemcpyHostToDevice, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+    }
+  }
+  for (lbm_sim* h : b->sims)
+    CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  int worst = LBM_OK;
+  for (lbm_sim* h : b->sims) {
+    int st = sticky_status(h);
+    if (st && !worst) worst = st;
+  }
+  return worst;
+}
+
+int lbm_batch_destroy(lbm_batch* b) {
+  if (!b) return LBM_E_INVALID;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (lbm_sim* h : b->sims) lbm_destroy(h);
+  dfree(b->d_sims);
+  dfree(b->d_pargs);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return LBM_OK;
+}
+
+}  // extern "C"

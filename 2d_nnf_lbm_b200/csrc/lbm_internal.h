@@ -206,6 +206,34 @@ cudaError_t launch_tile_order(const ParticleArgs& a, int buf, cudaStream_t s);
 cudaError_t launch_tiles_only(const ParticleArgs& a, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
+// Batched time steps (lbm_batch_*): many independent simulations advance in
+// one launch of the particle kernel (one block per simulation) and one of
+// the lattice kernel (a persistent grid over every simulation's tiles).
+struct BatchSim {
+  LatticeArgs a;       // the simulation's lattice arguments; src/dst, om_src/
+                       // om_dst, step and rec_slot are set on the device
+  void* f[2];
+  void* om[2];
+  long long* kk;       // step counter (the particle kernel increments it)
+  int* rec_slot;       // history slot of the step (written by the particle kernel)
+  int par0;            // f[(par0 + kk - 1) & 1] holds f*(kk) at lattice step kk
+  int nbx;             // tiles per row at the batch tile shape
+  long long first;     // first work item of this simulation
+};
+
+// Batch tile shapes (nodes): 0: 32 x 8, 1: 64 x 4, 2: 128 x 2.
+constexpr int BATCH_SHAPES = 3;
+__host__ __device__ constexpr int batch_bx(int shape) { return shape == 0 ? 32 : (shape == 1 ? 64 : 128); }
+__host__ __device__ constexpr int batch_by(int shape) { return 256 / batch_bx(shape); }
+
+cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, int shape,
+                              int grid, cudaStream_t s);
+cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
+                              int grid, cudaStream_t s);
+cudaError_t prepare_particles_batch();
+cudaError_t launch_particles_batch(const ParticleArgs* args, int nsim, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
 // Adjoint (reverse-mode) sweep, lbm_adjoint.cu.  Level n of the forward is
 // the step kernel that reads f*(n), omega(n) and the particle records of
 // step n and produces FORCE(n), f*(n+1), omega(n+1); the particle kernel of

@@ -562,9 +562,11 @@ __device__ __forceinline__ void facc_add(unsigned long long* hi, unsigned long l
 #define LBM_MINB_F64 1
 #endif
 
-template <class T, int MODE>
-__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_F32)
-    k_lattice(const LatticeArgs a) {
+// One tile of BX x BY nodes (block (bxi, byi) of the lattice), one node per
+// thread; BX*BY threads.  The tile lies inside one LTX x LTY list tile.
+template <class T, int MODE, int BX, int BY>
+__device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int byi) {
+  static_assert(LTX % BX == 0 && LTY % BY == 0 && BX % 32 == 0, "tile inside a list tile");
   constexpr bool F64 = sizeof(T) == 8;
   __shared__ int s_idx[MAX_TILE_CAND];
   __shared__ double s_px[MAX_TILE_CAND], s_py[MAX_TILE_CAND], s_pr[MAX_TILE_CAND];
@@ -572,9 +574,9 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int i = blockIdx.x * TX + (tid & (TX - 1));
-  const int j = blockIdx.y * TY + tid / TX;
-  const int tile = blockIdx.y * a.g.ltx + (blockIdx.x * TX) / LTX;
+  const int i = bxi * BX + (tid & (BX - 1));
+  const int j = byi * BY + tid / BX;
+  const int tile = ((byi * BY) / LTY) * a.g.ltx + (bxi * BX) / LTX;
   const Geometry& g = a.g;
   const Model& m = a.m;
   (void)warp;
@@ -642,9 +644,8 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
 #pragma unroll
       for (int k = 0; k < 9; ++k) f[k] = src[plane_of(k) * g.plane + n];
     } else {
-      const bool interior = blockIdx.x > 0 && blockIdx.y > 0 &&
-                            (int)(blockIdx.x + 1) * TX <= g.nx &&
-                            (int)(blockIdx.y + 1) * TY <= g.ny;
+      const bool interior = bxi > 0 && byi > 0 && (bxi + 1) * BX <= g.nx &&
+                            (byi + 1) * BY <= g.ny;
       const bool on_edge = i == 0 || i == g.nx || j == 0 || j == g.ny;
       if (interior)
         pull_interior<T>(src, g, n, f);
@@ -745,7 +746,7 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
   // ---- velocity correction (C1:1138-1152) --------------------------------
   const T uxc = ux + (T)0.5 * (gx + (T)0.0);
   const T uyc = uy + (T)0.5 * (gy + (T)0.0);
-  if ((MODE == MODE_INIT || MODE == MODE_RESTART) && m.bc == BC_EQUILIBRIUM && act)
+  if (MODE != MODE_OUTPUT && m.bc == BC_EQUILIBRIUM && act)
     ring_store<T>(a, i, j, (int)(a.step & 1), F64 ? rho : drho, uxc, uyc);
 
   if (MODE == MODE_OUTPUT) {
@@ -830,6 +831,12 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
     rec[2 * g.plane + n] = (T)no.t12;
     rec[3 * g.plane + n] = (T)no.yield;
   }
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_F32)
+    k_lattice(const LatticeArgs a) {
+  lattice_body<T, MODE, TX, TY>(a, blockIdx.x, blockIdx.y);
 }
 
 
@@ -1436,6 +1443,68 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kern, a, *tm);
+}
+
+// ---------------------------------------------------------------------------
+// Batched step: a persistent grid walks the work items (simulation, tile) of
+// every simulation in the batch, item = blockIdx.x + k*gridDim.x; a block
+// stages the arguments of the simulation it works on in shared memory, with
+// the ping-pong buffers, the step number and the history slot taken from the
+// simulation's device counters (so a captured graph replays unchanged).  The
+// node arithmetic is the scalar step's, so results do not depend on the tile
+// shape or the grid.
+template <class T, int BX, int BY>
+__global__ void __launch_bounds__(BX * BY)
+    k_lattice_batch(const BatchSim* __restrict__ sims, int nsim, long long total) {
+  __shared__ LatticeArgs s_a;
+  __shared__ int s_sim;
+  int cur = -1;
+  for (long long item = blockIdx.x; item < total; item += gridDim.x) {
+    __syncthreads();  // the previous tile is done with s_a and the candidates
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nsim - 1;  // last simulation with first <= item
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sims[mid].first <= item) lo = mid;
+        else hi = mid - 1;
+      }
+      s_sim = lo;
+    }
+    __syncthreads();
+    const int q = s_sim;
+    const BatchSim& B = sims[q];
+    if (q != cur) {
+      const int* src = reinterpret_cast<const int*>(&B.a);
+      int* dst = reinterpret_cast<int*>(&s_a);
+      for (int w = threadIdx.x; w < (int)(sizeof(LatticeArgs) / 4); w += BX * BY) dst[w] = src[w];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const long long k = *B.kk;
+        const int b = (int)((B.par0 + k - 1) & 1);
+        s_a.step = k;
+        s_a.rec_slot = *B.rec_slot;
+        s_a.src = B.f[b];
+        s_a.dst = B.f[b ^ 1];
+        s_a.om_src = B.om[b];
+        s_a.om_dst = B.om[b ^ 1];
+      }
+      __syncthreads();
+      cur = q;
+    }
+    const long long t = item - B.first;
+    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % B.nbx), (int)(t / B.nbx));
+  }
+}
+
+template <class T>
+cudaError_t launch_batch(const BatchSim* sims, int nsim, long long total, int shape, int grid,
+                         cudaStream_t s) {
+  switch (shape) {
+    case 0: k_lattice_batch<T, 32, 8><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+    case 1: k_lattice_batch<T, 64, 4><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+    default: k_lattice_batch<T, 128, 2><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+  }
+  return cudaGetLastError();
 }
 
 template <class T>

@@ -240,7 +240,16 @@ __device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
   }
 }
 
-__global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) {
+__device__ __forceinline__ void particles_body(const ParticleArgs& a);
+
+__global__ void __launch_bounds__(PBLK) k_particles(const ParticleArgs a) { particles_body(a); }
+
+// Batched: block b runs the particle step of simulation b.
+__global__ void __launch_bounds__(PBLK) k_particles_batch(const ParticleArgs* __restrict__ args) {
+  particles_body(args[blockIdx.x]);
+}
+
+__device__ __forceinline__ void particles_body(const ParticleArgs& a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PShared& S = *reinterpret_cast<PShared*>(smem_raw);
   __shared__ long long s_kk;
@@ -473,6 +482,18 @@ __global__ void __launch_bounds__(256) k_tiles_only(const ParticleArgs a) {
     a.tile_cur[0] = a.tile_cur[1] = 0;
     *a.pair_rebuild = 1;
   }
+}
+
+// The batched particle kernel's shared-memory size, set on the current
+// device before any launch (and so before any graph capture).
+cudaError_t prepare_particles_batch() {
+  return cudaFuncSetAttribute(k_particles_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(PShared));
+}
+
+cudaError_t launch_particles_batch(const ParticleArgs* args, int nsim, cudaStream_t s) {
+  k_particles_batch<<<nsim, PBLK, sizeof(PShared), s>>>(args);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {

@@ -270,6 +270,12 @@ def load_library():
         "lbm_strerror": ([ctypes.c_int], ctypes.c_char_p),
         "lbm_fields_noalloc": ([P(LbmParams), vp, ctypes.c_int32, vp, vp, vp], ctypes.c_int),
         "lbm_adjoint": ([vp, P(LbmObjective), dp, dp], ctypes.c_int),
+        "lbm_batch_create": ([P(LbmParams), ctypes.c_int32, P(vp)], ctypes.c_int),
+        "lbm_batch_sim": ([vp, ctypes.c_int32], vp),
+        "lbm_batch_step": ([vp, ctypes.c_int32], ctypes.c_int),
+        "lbm_batch_tuning": ([vp, ip, ip, ip], ctypes.c_int),
+        "lbm_batch_set_tuning": ([vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
+        "lbm_batch_destroy": ([vp], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -289,11 +295,16 @@ def _dptr(a: Optional[np.ndarray]):
 class Simulation:
     """One lattice + particle system on one GPU, driven through the C ABI."""
 
-    def __init__(self, params: LbmParams):
+    def __init__(self, params: LbmParams, _handle=None):
         self.lib = load_library()
         self.params = params.copy()
+        self._owned = _handle is None
         self._h = ctypes.c_void_p()
-        self._check(self.lib.lbm_create(ctypes.byref(self.params), ctypes.byref(self._h)), "lbm_create")
+        if _handle is None:
+            self._check(self.lib.lbm_create(ctypes.byref(self.params), ctypes.byref(self._h)),
+                        "lbm_create")
+        else:
+            self._h = ctypes.c_void_p(_handle)
         self.np = 0
         self.n1x, self.n1y = params.nx + 1, params.ny + 1
 
@@ -303,9 +314,9 @@ class Simulation:
             raise LbmError(rc, where, msg.decode() if msg else "")
 
     def close(self) -> None:
-        if self._h:
+        if self._h and self._owned:
             self.lib.lbm_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -431,3 +442,51 @@ class Simulation:
         per = g[LBM_GRAD_HEAD:LBM_GRAD_HEAD + LBM_GRAD_PER * self.np].reshape(-1, LBM_GRAD_PER)
         return v.value, {"tau_y": g[LBM_GRAD_TAU_Y], "nu": g[LBM_GRAD_NU],
                          "rho_p": per[:, 0].copy(), "x0": per[:, 1].copy(), "y0": per[:, 2].copy()}
+
+
+class Batch:
+    """lbm_batch_*: independent simulations advanced together, one launch per
+    kernel per step.  ``sims[i]`` is a Simulation view of simulation i (set
+    its particles, read its state); the batch owns the handles."""
+
+    def __init__(self, params_list):
+        self.lib = load_library()
+        arr = (LbmParams * len(params_list))(*[p.copy() for p in params_list])
+        self._b = ctypes.c_void_p()
+        rc = self.lib.lbm_batch_create(arr, len(params_list), ctypes.byref(self._b))
+        if rc != LBM_OK:
+            raise LbmError(rc, "lbm_batch_create")
+        self.sims = [Simulation(p, _handle=self.lib.lbm_batch_sim(self._b, i))
+                     for i, p in enumerate(params_list)]
+
+    def step(self, nsteps: int) -> None:
+        rc = self.lib.lbm_batch_step(self._b, int(nsteps))
+        if rc != LBM_OK:
+            raise LbmError(rc, "lbm_batch_step")
+
+    def tuning(self):
+        """(tile_x, tile_y, blocks_per_sm); zeros before the first step."""
+        v = [ctypes.c_int32() for _ in range(3)]
+        self.lib.lbm_batch_tuning(self._b, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
+    def set_tuning(self, tile_x: int, tile_y: int = 0, blocks_per_sm: int = 0) -> None:
+        rc = self.lib.lbm_batch_set_tuning(self._b, tile_x, tile_y, blocks_per_sm)
+        if rc != LBM_OK:
+            raise LbmError(rc, "lbm_batch_set_tuning")
+
+    def stream(self) -> int:
+        return self.sims[0].stream() if self.sims else 0
+
+    def close(self) -> None:
+        if self._b:
+            for s in self.sims:
+                s._h = ctypes.c_void_p()
+            self.lib.lbm_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

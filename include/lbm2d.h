@@ -280,6 +280,28 @@ typedef struct lbm_objective {
 } lbm_objective;
 int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, double* grads);
 
+/* Batched time steps (no counterpart in the reference, which runs one case
+ * per process): nsim independent simulations, each with its own lbm_params
+ * (lattice size, rheology, boundary, precision equal for all, device equal
+ * for all), advance together, one launch of the particle kernel (one block
+ * per simulation) and one of a persistent lattice kernel over every
+ * simulation's tiles per step, replayed from a captured CUDA graph.
+ * lbm_batch_sim returns simulation i's handle for everything else
+ * (lbm_set_particles, the getters, lbm_get_state ...); do not call
+ * lbm_step on it while it belongs to a batch.  The first lbm_batch_step
+ * picks the tile shape (32x8, 64x4 or 128x2 nodes) and the persistent grid
+ * (blocks per SM) by timing each on live steps; the results do not depend
+ * on the choice.  lbm_batch_set_tuning fixes them instead (tile_x 0:
+ * automatic).  The handles belong to the batch: lbm_batch_destroy destroys
+ * them. */
+typedef struct lbm_batch lbm_batch;
+int lbm_batch_create(const lbm_params* params, int32_t nsim, lbm_batch** out);
+lbm_sim* lbm_batch_sim(lbm_batch* b, int32_t i);
+int lbm_batch_step(lbm_batch* b, int32_t nsteps);
+int lbm_batch_tuning(lbm_batch* b, int32_t* tile_x, int32_t* tile_y, int32_t* blocks_per_sm);
+int lbm_batch_set_tuning(lbm_batch* b, int32_t tile_x, int32_t tile_y, int32_t blocks_per_sm);
+int lbm_batch_destroy(lbm_batch* b);
+
 /* Output fields of a state held in caller-owned device memory, computed
  * without allocating anything (no counterpart in the reference).
  *

@@ -1,0 +1,128 @@
+"""lbm_batch_*: simulations advanced together in one launch per kernel per
+step must reach, each of them, the state the same simulation reaches alone
+through lbm_step -- bit for bit in FP64 (same node arithmetic, exact force and
+mass sums); within 1e-6 of each quantity's scale in FP32, whose FP32
+translation unit lets the compiler contract products into FMAs differently
+in the batch kernel and the single-simulation kernel -- across graph
+replays, fresh starts and history draining; and bit for bit the same for
+every tile shape and grid in both precisions."""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import adjoint_cases as ac  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_cases(cases, precision):
+    out = []
+    for name in ("c6_bingham", "c1_newton", "c3_pair"):
+        p, pin, _, _ = ac.build(cases, name)
+        out.append((p.copy(precision=precision), pin))
+    p, pin = cases.shipped_c6(33, 97)  # odd sizes, the disk at its coded start
+    p.gravity = -1e-5
+    out.append((p.copy(precision=precision), pin))
+    p, pin = cases.shipped_c4(40, 30, 10.0, 10.0, 40.0)  # equilibrium boundary, prescribed motion
+    out.append((p.copy(precision=precision), pin))
+    p = cases.shipped_c1(48, 40, 8.0)  # no particles
+    out.append((p.copy(precision=precision), None))
+    for p, _ in out:
+        p.series_every = 5
+        p.series_capacity = 4  # the ring fills: the batch drains between chunks
+        p.series_particles = 2
+    return out
+
+
+def run_alone(pkg, p, pin, steps):
+    sim = pkg.Simulation(p)
+    if pin is not None:
+        sim.set_particles(pin)
+    sim.step(steps)
+    res = state(sim)
+    sim.close()
+    return res
+
+
+def state(sim):
+    return {
+        "parts": sim.particles() if sim.np else np.zeros(0),
+        "ux": sim.field("ux"),
+        "rho": sim.field("rho"),
+        "series": sim.series(),
+    }
+
+
+def assert_same(a, b, what):
+    for k in a:
+        assert np.array_equal(a[k], b[k], equal_nan=True), (what, k)
+
+
+def assert_close(a, b, what, rtol=1e-6):
+    for k in a:
+        x, y = np.nan_to_num(np.asarray(a[k])), np.nan_to_num(np.asarray(b[k]))
+        if k == "parts" and y.size:
+            cols = (slice(0, 2), slice(3, 6), slice(6, 9))  # position, velocity, force
+            for c in cols:
+                sc = max(float(np.max(np.abs(y[:, c]))), 1e-300)
+                assert np.max(np.abs(x[:, c] - y[:, c])) <= rtol * sc, (what, k, c)
+            continue
+        sc = max(float(np.max(np.abs(y))) if y.size else 0.0, 1e-300)
+        assert (np.max(np.abs(x - y)) if y.size else 0.0) <= rtol * sc, (what, k)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_matches_each_simulation_alone(pkg, cases, precision):
+    cs = mixed_cases(cases, precision)
+    steps = 53  # tuning steps, graph replays and a remainder
+    ref = [run_alone(pkg, p, pin, steps) for p, pin in cs]
+    b = pkg.Batch([p for p, _ in cs])
+    for s, (_, pin) in zip(b.sims, cs):
+        if pin is not None:
+            s.set_particles(pin)
+    b.step(20)
+    b.step(steps - 20)
+    tx, ty, bpsm = b.tuning()
+    assert tx * ty == 256 and bpsm > 0
+    for q, s in enumerate(b.sims):
+        if precision == 0:
+            assert_same(state(s), ref[q], (precision, q))
+        else:
+            assert_close(state(s), ref[q], (precision, q))
+    b.close()
+
+
+def batch_run(pkg, cs, shape, steps):
+    b = pkg.Batch([p for p, _ in cs])
+    b.set_tuning(*shape)
+    for s, (_, pin) in zip(b.sims, cs):
+        s.set_particles(pin)
+    b.step(steps)
+    assert b.tuning() == shape
+    out = [state(s) for s in b.sims]
+    b.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_tile_shapes_agree(pkg, cases, precision):
+    cs = mixed_cases(cases, precision)[:4]
+    ref = batch_run(pkg, cs, (32, 8, 2), 24)
+    for shape in ((64, 4, 4), (128, 2, 8), (32, 8, 1)):
+        got = batch_run(pkg, cs, shape, 24)
+        for q in range(len(cs)):
+            assert_same(got[q], ref[q], (shape, q))
+
+
+def test_batch_rejects_mixed_precision(pkg, cases):
+    p = cases.shipped_c1(40, 40, 8.0)
+    with pytest.raises(pkg.LbmError):
+        pkg.Batch([p.copy(precision=0), p.copy(precision=1)])
+    with pytest.raises(pkg.LbmError):
+        b = pkg.Batch([p])
+        b.set_tuning(48, 4, 2)
