@@ -340,6 +340,36 @@ def workload_cfg5(precision: int, bn: float = 5.0, nx=400, ny=1200, diam=24.0,
     return p, disk, {"u_ref": u_ref, "bn": bn, "n0": 3000, "n1": 4000}
 
 
+def workload_cfg4(precision: int, n: int = 256, seed: int = 0, tau_p: float = 0.9):
+    """Batched persistent solves: n independent Bingham single-disk settling
+    runs (the C6 program), seeded: width W ~ U[128, 512] lu (integer), height
+    3W, disk D = W/10 at (W/2, 3W - 7D), Bn log-uniform in [0.1, 100],
+    rho_p ~ U[1.2, 3.0], tau_p = 0.9, m = 1e5; gravity, U_REF and TAU_Y per
+    run as in the viscoplastic-settling workload (L_C = D).  Returns a list
+    of (params, disks)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        w = int(rng.integers(128, 513))
+        bn = float(10.0 ** rng.uniform(-1.0, 2.0))
+        rho_s = float(rng.uniform(1.2, 3.0))
+        diam = w / 10.0
+        p, _ = shipped_c6(w, 3 * w)
+        p.precision = precision
+        nu = r4((tau_p - 0.5) / 3.0)
+        re_s = r4(0.78)
+        a_g = -(re_s * nu * nu / ((diam ** 3) * (rho_s - 1.0) * 1.0))
+        u_ref = diam * diam * (rho_s - 1.0) * (-a_g) / nu
+        p.nu = nu
+        p.gravity = a_g
+        p.tau_y = bn * nu * u_ref / diam
+        p.m_pap = 1.0e5
+        p.c_ij = glowinski_cij(rho_s, 1.0, a_g, p.pi, diam)
+        disk = pin_array([[0.5 * w, 3.0 * w - 7.0 * diam]], diam, rho_s)
+        out.append((p, disk))
+    return out
+
+
 def mlups(nodes: int, steps: int, seconds: float) -> float:
     return nodes * steps / seconds / 1e6
 
@@ -359,6 +389,7 @@ __all__ = [
     "workload_cfg2",
     "workload_cfg2_particles",
     "workload_cfg3",
+    "workload_cfg4",
     "workload_cfg5",
     "mlups",
     "nodes_of",

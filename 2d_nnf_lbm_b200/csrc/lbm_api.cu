@@ -1774,6 +1774,12 @@ int lbm_batch_step(lbm_batch* b, int32_t nsteps) {
   return worst;
 }
 
+int lbm_batch_stream(lbm_batch* b, void** stream) {
+  if (!b || !stream) return LBM_E_INVALID;
+  *stream = b->stream;
+  return LBM_OK;
+}
+
 int lbm_batch_destroy(lbm_batch* b) {
   if (!b) return LBM_E_INVALID;
   cudaSetDevice(b->device);

@@ -1446,34 +1446,39 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
 }
 
 // ---------------------------------------------------------------------------
-// Batched step: a persistent grid walks the work items (simulation, tile) of
-// every simulation in the batch, item = blockIdx.x + k*gridDim.x; a block
-// stages the arguments of the simulation it works on in shared memory, with
-// the ping-pong buffers, the step number and the history slot taken from the
-// simulation's device counters (so a captured graph replays unchanged).  The
-// node arithmetic is the scalar step's, so results do not depend on the tile
+// Batched step: a persistent grid over the work items (simulation, tile) of
+// every simulation in the batch; block b takes a contiguous range of items,
+// so it stays inside one or two simulations.  When it enters a simulation it
+// stages that simulation's arguments in shared memory, with the ping-pong
+// buffers, the step number and the history slot taken from the simulation's
+// device counters (so a captured graph replays unchanged).  The node
+// arithmetic is the scalar step's, so results do not depend on the tile
 // shape or the grid.
 template <class T, int BX, int BY>
 __global__ void __launch_bounds__(BX * BY)
     k_lattice_batch(const BatchSim* __restrict__ sims, int nsim, long long total) {
   __shared__ LatticeArgs s_a;
   __shared__ int s_sim;
-  int cur = -1;
-  for (long long item = blockIdx.x; item < total; item += gridDim.x) {
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  const long long i0 = (long long)blockIdx.x * per;
+  const long long i1 = i0 + per < total ? i0 + per : total;
+  long long qfirst = 0, qend = -1;  // items of the staged simulation
+  int nbx = 1;
+  for (long long item = i0; item < i1; ++item) {
     __syncthreads();  // the previous tile is done with s_a and the candidates
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = nsim - 1;  // last simulation with first <= item
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (sims[mid].first <= item) lo = mid;
-        else hi = mid - 1;
+    if (item >= qend) {
+      if (threadIdx.x == 0) {
+        int lo = 0, hi = nsim - 1;  // last simulation with first <= item
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sims[mid].first <= item) lo = mid;
+          else hi = mid - 1;
+        }
+        s_sim = lo;
       }
-      s_sim = lo;
-    }
-    __syncthreads();
-    const int q = s_sim;
-    const BatchSim& B = sims[q];
-    if (q != cur) {
+      __syncthreads();
+      const int q = s_sim;
+      const BatchSim& B = sims[q];
       const int* src = reinterpret_cast<const int*>(&B.a);
       int* dst = reinterpret_cast<int*>(&s_a);
       for (int w = threadIdx.x; w < (int)(sizeof(LatticeArgs) / 4); w += BX * BY) dst[w] = src[w];
@@ -1489,10 +1494,12 @@ __global__ void __launch_bounds__(BX * BY)
         s_a.om_dst = B.om[b ^ 1];
       }
       __syncthreads();
-      cur = q;
+      qfirst = B.first;
+      qend = q + 1 < nsim ? sims[q + 1].first : total;
+      nbx = B.nbx;
     }
-    const long long t = item - B.first;
-    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % B.nbx), (int)(t / B.nbx));
+    const long long t = item - qfirst;
+    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % nbx), (int)(t / nbx));
   }
 }
 

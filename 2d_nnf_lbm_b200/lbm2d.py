@@ -276,6 +276,7 @@ def load_library():
         "lbm_batch_tuning": ([vp, ip, ip, ip], ctypes.c_int),
         "lbm_batch_set_tuning": ([vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
         "lbm_batch_destroy": ([vp], ctypes.c_int),
+        "lbm_batch_stream": ([vp, P(vp)], ctypes.c_int),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -475,8 +476,13 @@ class Batch:
         if rc != LBM_OK:
             raise LbmError(rc, "lbm_batch_set_tuning")
 
-    def stream(self) -> int:
-        return self.sims[0].stream() if self.sims else 0
+    def batch_stream(self) -> int:
+        """The batch's own cudaStream_t (as an integer)."""
+        s = ctypes.c_void_p()
+        rc = self.lib.lbm_batch_stream(self._b, ctypes.byref(s))
+        if rc != LBM_OK:
+            raise LbmError(rc, "lbm_batch_stream")
+        return int(s.value or 0)
 
     def close(self) -> None:
         if self._b:

@@ -22,6 +22,10 @@ workload (400x1200, one Bingham disk, 4000 steps, sqrt(N) checkpoints)
 against the forward time loop and checks its FP32 gradient against FP64
 central differences; --no-adjoint skips it.
 
+Batch (N=1): the "batch" object times lbm_batch_step on 256 independent
+Bingham single-disk runs of uneven sizes (--batch-steps steps) against the
+same runs one after another through lbm_step.
+
 Multi-GPU: the hot path does not shard (one simulation, one GPU); --gpus N
 runs N independent replicas (weak scaling), timed as the max over ranks.
 """
@@ -57,6 +61,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint/forward time measurement")
+    ap.add_argument("--batch-steps", type=int, default=1000,
+                    help="steps of the 256-simulation batch measurement (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="steps of the FP32-vs-FP64 trajectory comparison (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
@@ -384,6 +390,61 @@ def adjoint_measure(pkg, torch, device):
     return out
 
 
+def batch_measure(pkg, torch, device, steps):
+    """The batched workload (256 seeded Bingham single-disk runs, widths
+    128..512, heights 3x, FP32): one lbm_batch_step of `steps` steps (after
+    the tuning steps) against each run alone through lbm_step for the same
+    steps; CUDA events on the batch's / each handle's stream."""
+    cs = pkg.cases.workload_cfg4(1)
+    for p, _ in cs:
+        p.device = device
+    nodes = [(p.nx + 1) * (p.ny + 1) for p, _ in cs]
+    b = pkg.Batch([p for p, _ in cs])
+    for s, (_, pin) in zip(b.sims, cs):
+        s.set_particles(pin)
+    b.step(12)  # tuning (9 timed steps) and the first graph capture
+    ext = torch.cuda.ExternalStream(b.batch_stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(ext)
+    b.step(steps)
+    e1.record(ext)
+    e1.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    tuning = b.tuning()
+    finite = all(np.all(np.isfinite(s.particles())) for s in b.sims)
+    b.close()
+    alone = []
+    for p, pin in cs:
+        sim = pkg.Simulation(p)
+        sim.set_particles(pin)
+        sim.step(12)
+        ext = torch.cuda.ExternalStream(sim.stream())
+        torch.cuda.synchronize()
+        e0.record(ext)
+        sim.step(steps)
+        e1.record(ext)
+        e1.synchronize()
+        alone.append(e0.elapsed_time(e1))
+        sim.close()
+    alone = np.array(alone)
+    total = float(np.sum(nodes)) * steps
+    return {
+        "workload": "256 Bingham single-disk runs (C6), W ~ U[128,512], H = 3W, D = W/10, "
+                    "Bn log-uniform [0.1,100], rho_p ~ U[1.2,3], tau_p 0.9, m 1e5, seed 0, FP32",
+        "simulations": len(cs), "nodes": int(np.sum(nodes)), "steps": steps,
+        "tile": list(tuning[:2]), "blocks_per_sm": tuning[2],
+        "batch_ms": batch_ms, "batch_mlups": total / (batch_ms * 1e-3) / 1e6,
+        "per_sim_wall_ms_batched": batch_ms,
+        "sequential_ms": float(np.sum(alone)),
+        "sequential_mlups": total / (float(np.sum(alone)) * 1e-3) / 1e6,
+        "alone_ms_p50": float(np.percentile(alone, 50)), "alone_ms_p99": float(np.percentile(alone, 99)),
+        "speedup_vs_sequential": float(np.sum(alone)) / batch_ms,
+        "finite": bool(finite),
+    }
+
+
 def cpu_baseline(pkg, args, seconds):
     """The oracle (reference loop structure, one thread) on the same workload,
     timed over a bounded number of whole time steps."""
@@ -520,6 +581,8 @@ def main():
         line["trajectory_err"] = trajectory_error(pkg, args, device, args.accuracy_steps)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_measure(pkg, torch, device)
+    if world == 1 and args.batch_steps > 0:
+        line["batch"] = batch_measure(pkg, torch, device, args.batch_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pkg, args, args.cpu_seconds)
     if rank == 0:

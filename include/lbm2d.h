@@ -300,6 +300,8 @@ lbm_sim* lbm_batch_sim(lbm_batch* b, int32_t i);
 int lbm_batch_step(lbm_batch* b, int32_t nsteps);
 int lbm_batch_tuning(lbm_batch* b, int32_t* tile_x, int32_t* tile_y, int32_t* blocks_per_sm);
 int lbm_batch_set_tuning(lbm_batch* b, int32_t tile_x, int32_t tile_y, int32_t blocks_per_sm);
+/* The batch's CUDA stream (a cudaStream_t), for the caller's own events. */
+int lbm_batch_stream(lbm_batch* b, void** stream);
 int lbm_batch_destroy(lbm_batch* b);
 
 /* Output fields of a state held in caller-owned device memory, computed
