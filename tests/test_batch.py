@@ -67,10 +67,12 @@ def assert_close(a, b, what, rtol=1e-6):
     for k in a:
         x, y = np.nan_to_num(np.asarray(a[k])), np.nan_to_num(np.asarray(b[k]))
         if k == "parts" and y.size:
-            cols = (slice(0, 2), slice(3, 6), slice(6, 9))  # position, velocity, force
-            for c in cols:
+            # position, velocity; the hydrodynamic force, a sum over the disk
+            # with cancellation, gets ten times the tolerance
+            cols = ((slice(0, 2), rtol), (slice(3, 6), rtol), (slice(6, 9), 10 * rtol))
+            for c, tol in cols:
                 sc = max(float(np.max(np.abs(y[:, c]))), 1e-300)
-                assert np.max(np.abs(x[:, c] - y[:, c])) <= rtol * sc, (what, k, c)
+                assert np.max(np.abs(x[:, c] - y[:, c])) <= tol * sc, (what, k, c)
             continue
         sc = max(float(np.max(np.abs(y))) if y.size else 0.0, 1e-300)
         assert (np.max(np.abs(x - y)) if y.size else 0.0) <= rtol * sc, (what, k)
