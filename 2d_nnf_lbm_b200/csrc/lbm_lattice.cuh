@@ -1175,6 +1175,10 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
   const int pt = g.pitch;
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
+  // lane 0: this warp's fixed-point share of the mean-density sum, added to
+  // the history slot once when the warp leaves the loop (integer sums, so
+  // the total is the same as with one atomic per tile)
+  long long mass_q = 0;
 
   for (;; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
     if (!mbar_wait(full0 + 8 * sidx, (fpar >> sidx) & 1u, WAIT)) {
@@ -1326,10 +1330,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // ---- mean density at history steps (C1:318): fixed-point, order-free -
     if (rslot >= 0) {
       const double sd = warp_sum((double)drho);
-      if (lane == 0) {
-        const long long q = __double2ll_rn(sd * MASS_FIX);
-        atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
-      }
+      if (lane == 0) mass_q += __double2ll_rn(sd * MASS_FIX);
     }
     if (!act) continue;
 
@@ -1391,6 +1392,8 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       rec[3 * P + nd] = (T)no.yield;
     }
   }
+  if (rslot >= 0 && lane == 0 && mass_q != 0)
+    atomicAdd(a.mass_acc + rslot, (unsigned long long)mass_q);
 }
 
 // FP32: two CTAs per SM; FP64: one (with 17 warps, one SM sub-partition

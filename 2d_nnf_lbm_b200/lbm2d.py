@@ -370,13 +370,14 @@ class Simulation:
         ln = ctypes.c_int32()
         self._check(self.lib.lbm_series_record_len(self._h, ctypes.byref(ln)), "lbm_series_record_len")
         chunks = []
+        cap = min(4096, max(64, int(self.params.series_capacity)))
         while True:
-            buf = np.zeros((4096, ln.value))
+            buf = np.empty((cap, ln.value))
             n = ctypes.c_int32()
-            self._check(self.lib.lbm_get_series(self._h, _dptr(buf), 4096, ctypes.byref(n)), "lbm_get_series")
+            self._check(self.lib.lbm_get_series(self._h, _dptr(buf), cap, ctypes.byref(n)), "lbm_get_series")
             if n.value:
-                chunks.append(buf[: n.value].copy())
-            if n.value < 4096 or sum(len(c) for c in chunks) >= max_records:
+                chunks.append(buf[: n.value])
+            if n.value < cap or sum(len(c) for c in chunks) >= max_records:
                 break
         return np.concatenate(chunks) if chunks else np.zeros((0, ln.value))
 
