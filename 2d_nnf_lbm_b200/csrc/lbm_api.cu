@@ -11,6 +11,7 @@
 // demand without touching the state.
 #include <algorithm>
 #include <cmath>
+#include <deque>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -72,9 +73,21 @@ struct lbm_sim {
   int series_len = LBM_SERIES_HEAD;
   int series_cap = 0;
   int series_np = 0;
-  int64_t drained_kk = 0;
+  int64_t drained_kk = 0;      // records of steps <= drained_kk are in host_series
+  int64_t copied_kk = 0;       // records of steps <= copied_kk have their copies queued
   std::vector<double> host_series;
   size_t host_series_read = 0;
+  // pinned staging ring of the history records and their mean-density sums,
+  // filled by copies queued on the stream after the kernels that wrote them
+  double* series_pin = nullptr;              // [series_pcap][series_len]
+  unsigned long long* mass_pin = nullptr;    // [series_pcap]
+  int series_pcap = 0;
+  struct SeriesBatch {
+    long long r_end;  // records [drained record, r_end) complete with ev
+    cudaEvent_t ev;
+  };
+  std::deque<SeriesBatch> series_pending;
+  std::vector<cudaEvent_t> series_ev_free;
   // COMPUTEERROR: velocity of the previous call, per-block partial sums
   double* u0 = nullptr;       // [2][nodes]
   double* err_part = nullptr;
@@ -277,42 +290,86 @@ cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
   }
 }
 
-// Copy history records of steps (drained_kk, kk] from the device ring.
-int drain_series(lbm_sim* h) {
+// History records.  Record r (step (r+1)*every) sits in slot r % series_cap
+// of the device ring.  series_enqueue queues, on the handle's stream after
+// the kernels that wrote them, the copies of the records not yet queued into
+// the pinned staging ring (slot r % series_pcap), with their mean-density
+// sums, and clears those sums on the device; series_absorb_one waits for the
+// oldest queued batch only and moves it into host_series.
+int series_absorb_one(lbm_sim* h) {
+  const lbm_sim::SeriesBatch b = h->series_pending.front();
+  CK(cudaEventSynchronize(b.ev));
+  h->series_pending.pop_front();
+  h->series_ev_free.push_back(b.ev);
   const int every = h->p.series_every;
-  if (!h->series || every <= 0) {
-    h->drained_kk = h->kk;
-    return LBM_OK;
-  }
-  long long r0 = h->drained_kk / every, r1 = h->kk / every;  // records r0..r1-1
-  if (r1 <= r0) {
-    h->drained_kk = h->kk;
-    return LBM_OK;
-  }
-  CK(cudaStreamSynchronize(h->stream));
+  const long long r0 = h->drained_kk / every;
   const size_t len = (size_t)h->series_len;
   const size_t old = h->host_series.size();
-  h->host_series.resize(old + (size_t)(r1 - r0) * len);
+  h->host_series.resize(old + (size_t)(b.r_end - r0) * len);
   double* dst = h->host_series.data() + old;
-  std::vector<unsigned long long> acc;
-  long long r = r0;
   const double nn = (double)nodes(h);
-  while (r < r1) {
-    const long long slot = r % h->series_cap;
-    long long cnt = std::min<long long>(r1 - r, h->series_cap - slot);
-    CK(d2h(h, dst, h->series + slot * len, (size_t)cnt * len * sizeof(double)));
-    acc.resize(cnt);
-    CK(d2h(h, acc.data(), h->mass_acc + slot, (size_t)cnt * sizeof(unsigned long long)));
-    // the slots start at zero again before the ring comes back to them
-    CK(cudaMemsetAsync(h->mass_acc + slot, 0, (size_t)cnt * sizeof(unsigned long long), h->stream));
+  for (long long r = r0; r < b.r_end; ++r, dst += len) {
+    const long long ps = r % h->series_pcap;
+    std::memcpy(dst, h->series_pin + ps * len, len * sizeof(double));
     // AvgDen = rho0 + sum(rho - rho0)/N from the fixed-point accumulator
-    for (long long q = 0; q < cnt; ++q)
-      dst[q * len + 1] = h->p.rho0 + (double)(long long)acc[q] / MASS_FIX / nn;
-    dst += cnt * len;
+    dst[1] = h->p.rho0 + (double)(long long)h->mass_pin[ps] / MASS_FIX / nn;
+  }
+  h->drained_kk = b.r_end * every;
+  return LBM_OK;
+}
+
+int series_enqueue(lbm_sim* h) {
+  const int every = h->p.series_every;
+  if (!h->series || every <= 0) {
+    h->copied_kk = h->drained_kk = h->kk;
+    return LBM_OK;
+  }
+  const long long r0 = h->copied_kk / every, r1 = h->kk / every;
+  if (r1 <= r0) return LBM_OK;
+  int rc;
+  while (!h->series_pending.empty() && r1 - h->drained_kk / every > h->series_pcap)
+    if ((rc = series_absorb_one(h))) return rc;
+  const size_t len = (size_t)h->series_len;
+  const long long cap = h->series_cap, pcap = h->series_pcap;
+  for (long long r = r0; r < r1;) {
+    const long long ds = r % cap, ps = r % pcap;
+    const long long cnt = std::min(r1 - r, std::min(cap - ds, pcap - ps));
+    CK(cudaMemcpyAsync(h->series_pin + ps * len, h->series + ds * len, cnt * len * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->mass_pin + ps, h->mass_acc + ds, cnt * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, h->stream));
+    // the slots start at zero again before the ring comes back to them
+    CK(cudaMemsetAsync(h->mass_acc + ds, 0, cnt * sizeof(unsigned long long), h->stream));
     r += cnt;
   }
-  h->drained_kk = h->kk;
+  cudaEvent_t ev = nullptr;
+  if (!h->series_ev_free.empty()) {
+    ev = h->series_ev_free.back();
+    h->series_ev_free.pop_back();
+  } else {
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  CK(cudaEventRecord(ev, h->stream));
+  h->series_pending.push_back({r1, ev});
+  h->copied_kk = r1 * every;
   return LBM_OK;
+}
+
+// Every record of steps up to kk into host_series.
+int drain_series(lbm_sim* h) {
+  int rc = series_enqueue(h);
+  if (rc) return rc;
+  while (!h->series_pending.empty())
+    if ((rc = series_absorb_one(h))) return rc;
+  return LBM_OK;
+}
+
+// Drop the queued batches (their copies have completed: callers synchronise
+// the stream first) and the records not yet drained.
+void series_reset(lbm_sim* h, long long kk) {
+  for (const auto& b : h->series_pending) h->series_ev_free.push_back(b.ev);
+  h->series_pending.clear();
+  h->drained_kk = h->copied_kk = kk;
 }
 
 // Fields of step kk in h->out (and F after BC in h->out_f when want_f).
@@ -337,6 +394,14 @@ int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
   dfree(h->series); dfree(h->mass_acc);
   h->ps = nullptr; h->facc = nullptr; h->nbr = nullptr; h->nbr_count = nullptr;
   h->nbr_xy = nullptr; h->series = nullptr; h->mass_acc = nullptr;
+  // records of the old disk set (its record length) are dropped
+  series_reset(h, h->kk);
+  h->host_series.clear();
+  h->host_series_read = 0;
+  if (h->series_pin) cudaFreeHost(h->series_pin);
+  if (h->mass_pin) cudaFreeHost(h->mass_pin);
+  h->series_pin = nullptr;
+  h->mass_pin = nullptr;
   h->np = np;
   h->partials_valid = false;
   // pair search cells cover the Verlet radius D_max + repulsion range + SKIN
@@ -363,6 +428,14 @@ int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
     if ((rc = dalloc(&h->series, (size_t)h->series_cap * h->series_len))) return rc;
     if ((rc = dalloc(&h->mass_acc, (size_t)h->series_cap))) return rc;
     CK(cudaMemsetAsync(h->mass_acc, 0, sizeof(unsigned long long) * h->series_cap, h->stream));
+    h->series_pcap = 2 * h->series_cap;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&h->series_pin),
+                      sizeof(double) * h->series_pcap * h->series_len, cudaHostAllocDefault) !=
+            cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&h->mass_pin),
+                      sizeof(unsigned long long) * h->series_pcap, cudaHostAllocDefault) !=
+            cudaSuccess)
+      return LBM_E_NOMEM;
   }
   return LBM_OK;
 }
@@ -536,6 +609,10 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->d_kk); dfree(h->stale_dpw);
   dfree(h->series); dfree(h->out); dfree(h->out_f); dfree(h->d_status);
   dfree(h->u0); dfree(h->err_part);
+  if (h->series_pin) cudaFreeHost(h->series_pin);
+  if (h->mass_pin) cudaFreeHost(h->mass_pin);
+  for (const auto& b : h->series_pending) cudaEventDestroy(b.ev);
+  for (cudaEvent_t e : h->series_ev_free) cudaEventDestroy(e);
   dfree(h->adj_slots); dfree(h->adj_ck); dfree(h->adj_ckp); dfree(h->adj_hist);
   for (int b = 0; b < 2; ++b) {
     dfree(h->adj_a[b]);
@@ -583,8 +660,8 @@ __global__ void __launch_bounds__(ERR_TPB) k_error(const double* ux, const doubl
 // kernel (the body of lbm_step's loop).
 int enqueue_step(lbm_sim* h) {
   const int every = h->p.series_every;
-  if (h->series && every > 0 && (h->kk + 1) / every - h->drained_kk / every > h->series_cap) {
-    int rc = drain_series(h);
+  if (h->series && every > 0 && (h->kk + 1) / every - h->copied_kk / every > h->series_cap) {
+    int rc = series_enqueue(h);  // stream-ordered: the ring slots are copied before reuse
     if (rc) return rc;
   }
   if (h->prof) {
@@ -885,7 +962,7 @@ int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
   if ((rc = launch_tiles(h))) return rc;
   CK(cudaStreamSynchronize(h->stream));
   h->out_kk = -1;
-  h->drained_kk = h->kk;
+  series_reset(h, h->kk);
   return refreshed_status(h);
 }
 
@@ -896,6 +973,10 @@ int lbm_step(lbm_sim* h, int32_t nsteps) {
   cudaSetDevice(h->p.device);
   for (int32_t s = 0; s < nsteps; ++s) {
     int rc = enqueue_step(h);
+    if (rc) return rc;
+  }
+  if (h->series) {
+    int rc = series_enqueue(h);  // this call's records, copied behind its kernels
     if (rc) return rc;
   }
   h->out_kk = -1;
@@ -1000,9 +1081,14 @@ int lbm_series_record_len(lbm_sim* h, int32_t* len) {
 int lbm_get_series(lbm_sim* h, double* out, int32_t max_records, int32_t* nrec) {
   if (!h || !nrec || max_records < 0) return LBM_E_INVALID;
   cudaSetDevice(h->p.device);
-  int rc = drain_series(h);
-  if (rc) return rc;
   const size_t len = (size_t)h->series_len;
+  // wait only for the oldest batches the request needs: steps queued after
+  // them keep running while the caller reads these
+  int rc = series_enqueue(h);
+  if (rc) return rc;
+  while ((h->host_series.size() - h->host_series_read) / len < (size_t)max_records &&
+         !h->series_pending.empty())
+    if ((rc = series_absorb_one(h))) return rc;
   const size_t avail = (h->host_series.size() - h->host_series_read) / len;
   const size_t n = std::min<size_t>(avail, (size_t)max_records);
   if (n && out)
@@ -1013,7 +1099,7 @@ int lbm_get_series(lbm_sim* h, double* out, int32_t max_records, int32_t* nrec) 
     h->host_series_read = 0;
   }
   *nrec = (int32_t)n;
-  return refreshed_status(h);
+  return sticky_status(h);  // as of the last lbm_step; no wait for later steps
 }
 
 int lbm_get_mean_density(lbm_sim* h, double* avg) {
@@ -1114,7 +1200,7 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, 
     CK(cudaStreamSynchronize(h->stream));
   }
   h->kk = kk;
-  h->drained_kk = kk;
+  series_reset(h, kk);
   h->host_series.clear();
   h->host_series_read = 0;
   if ((rc = launch_tiles(h))) return rc;

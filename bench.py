@@ -246,7 +246,8 @@ def run_e2e(pkg, torch, args, device):
     record -- per disk x, y, angle, u, v, omega, FORCE, F_H_IN, and the mean
     density, what the reference writes every step (C1:264, C1:318) -- copied
     to host memory: the library keeps the records in a device ring and
-    lbm_get_series drains them every E2E_CHUNK steps."""
+    lbm_get_series drains them every E2E_CHUNK steps, each chunk's records
+    read while the next chunk runs."""
     p, pin = workload(pkg, 1, args)
     p.device = device
     p.series_every = 1
@@ -265,15 +266,15 @@ def run_e2e(pkg, torch, args, device):
     w0 = time.perf_counter()
     t0.record(ext)
     sim.set_particles(pin_h)
-    got = 0
+    chunks = [min(E2E_CHUNK, k - s0) for s0 in range(0, k, E2E_CHUNK)]
     rec_len = 0
-    while got < k:
-        c = min(E2E_CHUNK, k - got)
-        sim.step(c)
-        rec = sim.series()
+    sim.step(chunks[0])
+    for i, c in enumerate(chunks):
+        if i + 1 < len(chunks):
+            sim.step(chunks[i + 1])  # queued before this chunk's records are read
+        rec = sim.series(max_records=c)
         assert rec.shape[0] == c, (rec.shape, c)
         rec_len = rec.shape[1]
-        got += c
     t1.record(ext)
     t1.synchronize()
     wall = time.perf_counter() - w0
