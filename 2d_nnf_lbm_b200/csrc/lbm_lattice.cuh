@@ -564,8 +564,12 @@ __device__ __forceinline__ void facc_add(unsigned long long* hi, unsigned long l
 
 // One tile of BX x BY nodes (block (bxi, byi) of the lattice), one node per
 // thread; BX*BY threads.  The tile lies inside one LTX x LTY list tile.
+// mass_local (MODE_STEP): when given, lane 0 adds the warp's fixed-point
+// mean-density share there instead of to the history slot (the caller adds
+// the total once); integer sums, so the result is the same.
 template <class T, int MODE, int BX, int BY>
-__device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int byi) {
+__device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int byi,
+                                             long long* mass_local = nullptr) {
   static_assert(LTX % BX == 0 && LTY % BY == 0 && BX % 32 == 0, "tile inside a list tile");
   constexpr bool F64 = sizeof(T) == 8;
   __shared__ int s_idx[MAX_TILE_CAND];
@@ -774,7 +778,8 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
     double s0 = warp_sum((double)drho);
     if (lane == 0) {
       const long long q = __double2ll_rn(s0 * MASS_FIX);
-      atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
+      if (mass_local) *mass_local += q;
+      else atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
     }
   }
 
@@ -1467,9 +1472,16 @@ __global__ void __launch_bounds__(BX * BY)
   const long long i1 = i0 + per < total ? i0 + per : total;
   long long qfirst = 0, qend = -1;  // items of the staged simulation
   int nbx = 1;
+  // lane 0: the warp's mean-density share for the staged simulation's
+  // history slot, added once when the block leaves the simulation
+  long long mass_q = 0;
+  unsigned long long* mass_ptr = nullptr;
   for (long long item = i0; item < i1; ++item) {
     __syncthreads();  // the previous tile is done with s_a and the candidates
     if (item >= qend) {
+      if ((threadIdx.x & 31) == 0 && mass_ptr && mass_q)
+        atomicAdd(mass_ptr, (unsigned long long)mass_q);
+      mass_q = 0;
       if (threadIdx.x == 0) {
         int lo = 0, hi = nsim - 1;  // last simulation with first <= item
         while (lo < hi) {
@@ -1500,10 +1512,12 @@ __global__ void __launch_bounds__(BX * BY)
       qfirst = B.first;
       qend = q + 1 < nsim ? sims[q + 1].first : total;
       nbx = B.nbx;
+      mass_ptr = (s_a.rec_slot >= 0 && s_a.mass_acc) ? s_a.mass_acc + s_a.rec_slot : nullptr;
     }
     const long long t = item - qfirst;
-    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % nbx), (int)(t / nbx));
+    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % nbx), (int)(t / nbx), &mass_q);
   }
+  if ((threadIdx.x & 31) == 0 && mass_ptr && mass_q) atomicAdd(mass_ptr, (unsigned long long)mass_q);
 }
 
 template <class T>
