@@ -1042,15 +1042,31 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // disks waits for it (griddepcontrol.wait), and by then every
     // particle-free tile has been handed out.  Taking tiles one at a time
     // from the queue keeps the CTAs finishing together.
-    int bo = 0;
-    if (lane == 0) bo = a.tile_cur[(a.step - 1) & 1];
-    const int buf_old = __shfl_sync(0xffffffffu, bo, 0);
-    int nu = 0;
-    if (lane == 0) nu = a.n_unlisted[buf_old];
-    const int* order = a.tile_order + (long long)buf_old * a.ntiles;
     int* ctr = a.work_ctr + (a.step & 1);
     constexpr int SX = LTX / ST::TW, SY = LTY / ST::TR, S = SX * SY;  // step tiles per list tile
     const int Q = S * a.ntiles;
+    // Queue entries blockIdx.x and gridDim.x + blockIdx.x are this CTA's
+    // without an atomic; the shared counter hands out the rest from 2 x grid
+    // on.  The list buffer of the previous step, its order and unlisted count
+    // are read together with both buffers' candidates for those two entries,
+    // so the first TMA issue waits for one round trip.
+    const int base = 2 * (int)gridDim.x;
+    int t0 = (int)blockIdx.x, t1 = (int)gridDim.x + (int)blockIdx.x, t2 = 0;
+    int L0 = 0, L1 = 0, L2 = 0, nu = 0, bo = 0;
+    if (lane == 0) {
+      const int* o0 = a.tile_order;
+      const int* o1 = a.tile_order + a.ntiles;
+      bo = a.tile_cur[(a.step - 1) & 1];
+      const int nu0 = a.n_unlisted[0], nu1 = a.n_unlisted[1];
+      const int a0 = t0 < Q ? o0[t0 / S] : 0, a1 = t0 < Q ? o1[t0 / S] : 0;
+      const int b0 = t1 < Q ? o0[t1 / S] : 0, b1 = t1 < Q ? o1[t1 / S] : 0;
+      t2 = base + atomicAdd(ctr, 1);
+      nu = bo ? nu1 : nu0;
+      L0 = bo ? a1 : a0;
+      L1 = bo ? b1 : b0;
+    }
+    const int buf_old = __shfl_sync(0xffffffffu, bo, 0);
+    const int* order = a.tile_order + (long long)buf_old * a.ntiles;
     int buf = -1;
     bool waited = false;
     int sidx = 0;
@@ -1126,28 +1142,20 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // that rotate through "take" (atomicAdd issued), "look up" (order load
     // issued) and "issue", so neither latency is waited for while the ring
     // has work.
-    int t0 = 0, L0 = 0, t1 = 0, L1 = 0, t2 = 0, L2 = 0;
-    if (lane == 0) {
-      t0 = atomicAdd(ctr, 2);
-      t1 = t0 + 1;
-      L0 = t0 < Q ? order[t0 / S] : 0;
-    }
     for (;;) {
-      if (lane == 0) {
-        L1 = t1 < Q ? order[t1 / S] : 0;
-        t2 = atomicAdd(ctr, 1);
-      }
+      if (lane == 0) L2 = t2 < Q ? order[t2 / S] : 0;
       if (!issue(__shfl_sync(0xffffffffu, t0, 0), __shfl_sync(0xffffffffu, L0, 0))) break;
-      if (lane == 0) {
-        L2 = t2 < Q ? order[t2 / S] : 0;
-        t0 = atomicAdd(ctr, 1);
-      }
+      if (lane == 0) t0 = base + atomicAdd(ctr, 1);
       if (!issue(__shfl_sync(0xffffffffu, t1, 0), __shfl_sync(0xffffffffu, L1, 0))) break;
       if (lane == 0) {
         L0 = t0 < Q ? order[t0 / S] : 0;
-        t1 = atomicAdd(ctr, 1);
+        t1 = base + atomicAdd(ctr, 1);
       }
       if (!issue(__shfl_sync(0xffffffffu, t2, 0), __shfl_sync(0xffffffffu, L2, 0))) break;
+      if (lane == 0) {
+        L1 = t1 < Q ? order[t1 / S] : 0;
+        t2 = base + atomicAdd(ctr, 1);
+      }
     }
     if (alive) {
       // end marker: a stage whose tile column is -1

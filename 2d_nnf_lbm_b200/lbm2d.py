@@ -381,6 +381,21 @@ class Simulation:
                 break
         return np.concatenate(chunks) if chunks else np.zeros((0, ln.value))
 
+    def series_into(self, out: np.ndarray) -> int:
+        """lbm_get_series into a caller-kept C-contiguous float64 array of
+        shape (records, record length); returns the number of records read."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.ndim != 2:
+            raise ValueError("out must be a C-contiguous 2-D float64 array")
+        n = ctypes.c_int32()
+        self._check(self.lib.lbm_get_series(self._h, _dptr(out), out.shape[0], ctypes.byref(n)),
+                    "lbm_get_series")
+        return n.value
+
+    def series_record_len(self) -> int:
+        ln = ctypes.c_int32()
+        self._check(self.lib.lbm_series_record_len(self._h, ctypes.byref(ln)), "lbm_series_record_len")
+        return ln.value
+
     def mean_density(self) -> float:
         v = ctypes.c_double()
         self._check(self.lib.lbm_get_mean_density(self._h, ctypes.byref(v)), "lbm_get_mean_density")
