@@ -35,6 +35,7 @@ struct lbm_sim {
   size_t esz = 8;
   void* f[2] = {nullptr, nullptr};
   void* om[2] = {nullptr, nullptr};
+  void* pm[2] = {nullptr, nullptr};  // previous-collision macros (BGK bi-viscosity)
   void* rec = nullptr;
   void* ring = nullptr;  // equilibrium boundary: T[2][3][ring_n]
   int ring_n = 0;
@@ -191,6 +192,8 @@ LatticeArgs lattice_args(lbm_sim* h) {
   a.dst = h->f[h->cur ^ 1];
   a.om_src = h->om[h->cur];
   a.om_dst = h->om[h->cur ^ 1];
+  a.pm_src = h->pm[h->cur];
+  a.pm_dst = h->pm[h->cur ^ 1];
   a.ps = h->ps;
   a.np = h->np;
   a.npad = h->npad;
@@ -274,6 +277,10 @@ ParticleArgs particle_args(lbm_sim* h) {
 }
 
 cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
+  // the BGK collision (C1:774-841) runs in the one-node-per-thread step
+  if (mode == 0 && h->m.bgk)
+    return h->prec == LBM_FP64 ? launch_bgk_step_fp64(a, h->stream)
+                               : launch_bgk_step_fp32(a, h->stream);
   if (h->prec == LBM_FP64) {
     switch (mode) {
       case 0: return launch_step_fp64(a, &h->tm[h->cur], h->stream);
@@ -598,6 +605,7 @@ void destroy_buffers(lbm_sim* h) {
   for (int b = 0; b < 2; ++b) {
     dfree(h->f[b]);
     dfree(h->om[b]);
+    dfree(h->pm[b]);
   }
   dfree(h->rec);
   dfree(h->ring);
@@ -782,6 +790,8 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
     return LBM_E_INVALID;
   if (p.motion != LBM_MOTION_FREE && p.motion != LBM_MOTION_OSCILLATE) return LBM_E_INVALID;
   if (p.strain_model != LBM_STRAIN_MEQ && p.strain_model != LBM_STRAIN_FEQ) return LBM_E_INVALID;
+  if (p.collision != LBM_COLLISION_MRT && p.collision != LBM_COLLISION_BGK) return LBM_E_INVALID;
+  if (p.collision == LBM_COLLISION_BGK && p.rheology == LBM_CASSON) return LBM_E_INVALID;
   if (p.motion == LBM_MOTION_OSCILLATE && (!std::isfinite(p.osc_u) || !(p.osc_period > 0.0)))
     return LBM_E_INVALID;
   if (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM && p.rheology != LBM_CASSON)
@@ -857,6 +867,18 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
     const double W = p.w_init[k == 0 ? 0 : (k < 5 ? 1 : 2)];
     m.eq_c_f[k] = (float)(p.rho0 * (W * (k < 5 ? 2.0 : 1.0) - w[k]));
   }
+  // COLLISION (C1:774-841): MU_R = 1000.0*MU_0, GAMMA_C = TAU_Y/(MU_R-MU_0)
+  // (C1:49-53, MU_0 = NU); the forcing weights of ComputeSourceEquilib_Hydro
+  // are REAL(4) quotients (C1:847)
+  m.bgk = p.collision == LBM_COLLISION_BGK;
+  m.mu_r = 1000.0 * p.nu;
+  m.gamma_c = p.tau_y / (m.mu_r - p.nu);
+  m.w_src[0] = (double)(4.0f / 9.0f);
+  m.w_src[1] = (double)(1.0f / 9.0f);
+  m.w_src[2] = (double)(1.0f / 36.0f);
+  m.mu_r_f = (float)m.mu_r;
+  m.gamma_c_f = (float)m.gamma_c;
+  for (int k = 0; k < 3; ++k) m.w_src_f[k] = (float)m.w_src[k];
 
   int rc = LBM_OK;
   auto fail = [&](int code) {
@@ -876,6 +898,8 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   for (int b = 0; b < 2; ++b) {
     if (cudaMalloc(&h->f[b], fbytes) != cudaSuccess) return fail(LBM_E_NOMEM);
     if (m.bingham && cudaMalloc(&h->om[b], (size_t)h->g.plane * h->esz) != cudaSuccess)
+      return fail(LBM_E_NOMEM);
+    if (m.bgk && m.bingham && cudaMalloc(&h->pm[b], (size_t)3 * h->g.plane * h->esz) != cudaSuccess)
       return fail(LBM_E_NOMEM);
   }
   if (m.record_stress &&
@@ -923,6 +947,7 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   a.src = nullptr;
   a.dst = h->f[0];
   a.om_dst = h->om[0];
+  a.pm_dst = h->pm[0];
   if (launch_lattice(h, a, 2) != cudaSuccess) return fail(LBM_E_CUDA);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return fail(LBM_E_CUDA);
   *out = h;
@@ -1236,6 +1261,7 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega, 
   a.om_src = h->om[prev];
   a.dst = h->f[h->cur];
   a.om_dst = h->om[h->cur];
+  a.pm_dst = h->pm[h->cur];
   CK(launch_lattice(h, a, 3));
   CK(cudaStreamSynchronize(h->stream));
   h->prev_post_bc = true;
@@ -1490,6 +1516,7 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
   if ((p.bc != LBM_BC_ZOUHE && p.bc != LBM_BC_HALFWAY_BB) ||
       (p.rheology != LBM_NEWTONIAN && p.rheology != LBM_BINGHAM) ||
       p.strain_model != LBM_STRAIN_MEQ || p.motion != LBM_MOTION_FREE ||
+      p.collision != LBM_COLLISION_MRT ||
       (h->np > 1 && p.contact_test != LBM_CONTACT_DPP))
     return LBM_E_INVALID;
   int st = sticky_status(h);
@@ -1652,6 +1679,7 @@ int batch_upload(lbm_batch* b, int shape) {
     for (int k = 0; k < 2; ++k) {
       B.f[k] = h->f[k];
       B.om[k] = h->om[k];
+      B.pm[k] = h->pm[k];
     }
     B.kk = h->d_kk;
     B.rec_slot = h->rec_slot;

@@ -19,4 +19,7 @@ cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, i
                               int grid, cudaStream_t s) {
   return launch_batch<float>(sims, nsim, total, shape, grid, s);
 }
+cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<float>(a, s, MODE_STEP);
+}
 }  // namespace lbm

@@ -21,4 +21,7 @@ cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, i
                               int grid, cudaStream_t s) {
   return launch_batch<double>(sims, nsim, total, shape, grid, s);
 }
+cudaError_t launch_bgk_step_fp64(const LatticeArgs& a, cudaStream_t s) {
+  return launch_mode<double>(a, s, MODE_STEP);
+}
 }  // namespace lbm

@@ -104,6 +104,12 @@ struct Model {
   // equilibrium boundary in FP32: COMPUTEFEQNEW weights and, per k,
   // rho0*(W_k*B_k(u=0) - w_k) of the shifted form
   float w_init_f[3], eq_c_f[9];
+  // LBM_COLLISION_BGK (COLLISION, C1:774-841): bi-viscosity MU_R = 1000 nu,
+  // GAMMA_C = tau_y/(MU_R - nu); ComputeSourceEquilib_Hydro's forcing weights
+  // (the REAL(4) quotients 4/9, 1/9, 1/36)
+  int bgk;
+  double mu_r, gamma_c, w_src[3];
+  float mu_r_f, gamma_c_f, w_src_f[3];
 };
 
 struct ParticleArgs {
@@ -154,6 +160,10 @@ struct LatticeArgs {
   void* dst;             // f written
   const void* om_src;
   void* om_dst;
+  // LBM_COLLISION_BGK with a Bingham rheology: the density (FP32: rho - rho0)
+  // and corrected velocity of each node's previous collision, T[3][plane]
+  const void* pm_src;
+  void* pm_dst;
   const double* ps;      // [PS][npad]
   int np, npad;
   const int* tile_count; // [2][ntiles]
@@ -191,6 +201,9 @@ cudaError_t launch_init_fp32(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s);
 cudaError_t launch_output_fp32(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s);
+// One time step of the BGK collision (one node per thread).
+cudaError_t launch_bgk_step_fp64(const LatticeArgs& a, cudaStream_t s);
+cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s);
 
 // TMA box of the step kernel: one tile row (128 FP32 / 64 FP64 nodes) plus
 // a 16-byte vector of halo on each side; 512 / row-width rows; one plane.
@@ -214,6 +227,7 @@ struct BatchSim {
                        // om_dst, step and rec_slot are set on the device
   void* f[2];
   void* om[2];
+  void* pm[2];         // previous-collision macros (BGK bi-viscosity), or null
   long long* kk;       // step counter (the particle kernel increments it)
   int* rec_slot;       // history slot of the step (written by the particle kernel)
   int par0;            // f[(par0 + kk - 1) & 1] holds f*(kk) at lattice step kk

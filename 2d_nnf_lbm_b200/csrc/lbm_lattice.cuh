@@ -87,6 +87,46 @@ __device__ __forceinline__ void ring_store(const LatticeArgs& a, int i, int j, i
   }
 }
 
+// COMPUTEFEQNEW (C1:1157-1175) in the FP32 shifted form, from dr = rho - rho0:
+// h_k = W_k (dr B_k + rho0 (B_k - B_k(0))) + rho0 (W_k B_k(0) - w_k), B_k the
+// bracket of COMPUTEFEQNEW, so no O(1) terms cancel.
+__device__ __forceinline__ void feq_shift32(const Model& m, float dr, float x, float y, float* h) {
+  const float r0 = m.rho0_f;
+  const float U2 = x * x + y * y;
+  float d[9];  // B_k - B_k(0)
+  d[0] = -3.f * U2;
+  d[1] = 6.f * x + 9.f * x * x - 3.f * U2;
+  d[2] = 6.f * y + 9.f * y * y - 3.f * U2;
+  d[3] = -6.f * x + 9.f * x * x - 3.f * U2;
+  d[4] = -6.f * y + 9.f * y * y - 3.f * U2;
+  d[5] = 3.f * (x + y) + 9.f * x * y + 3.f * U2;
+  d[6] = -3.f * (x - y) - 9.f * x * y + 3.f * U2;
+  d[7] = -3.f * (x + y) + 9.f * x * y + 3.f * U2;
+  d[8] = 3.f * (x - y) - 9.f * x * y + 3.f * U2;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const float W = m.w_init_f[k == 0 ? 0 : (k < 5 ? 1 : 2)];
+    const float B = (k == 0 || k < 5 ? 2.f : 1.f) + d[k];
+    h[k] = W * (dr * B + r0 * d[k]) + m.eq_c_f[k];
+  }
+}
+
+// ComputeSourceEquilib_Hydro's forcing (C1:843-870, G_X = G_Y = 0).
+template <class T>
+__device__ __forceinline__ void bgk_source(const T* W, T rho, T ux, T uy, T gx, T gy, T* FI) {
+  gx = gx + (T)0.0;
+  gy = gy + (T)0.0;
+  FI[0] = W[0] * rho * (-((T)3 * ux * gx) - (T)3 * uy * gy);
+  FI[1] = W[1] * rho * (((T)3 + (T)6 * ux) * gx - (T)3 * uy * gy);
+  FI[2] = W[1] * rho * (-((T)3 * ux * gx) + ((T)3 + (T)6 * uy) * gy);
+  FI[3] = W[1] * rho * (((T)-3 + (T)6 * ux) * gx - (T)3 * uy * gy);
+  FI[4] = W[1] * rho * (-((T)3 * ux * gx) + ((T)-3 + (T)6 * uy) * gy);
+  FI[5] = W[2] * rho * (((T)3 + (T)6 * ux + (T)9 * uy) * gx + ((T)3 + (T)9 * ux + (T)6 * uy) * gy);
+  FI[6] = W[2] * rho * (((T)-3 + (T)6 * ux - (T)9 * uy) * gx + ((T)3 - (T)9 * ux + (T)6 * uy) * gy);
+  FI[7] = W[2] * rho * (((T)-3 + (T)6 * ux + (T)9 * uy) * gx + ((T)-3 + (T)9 * ux + (T)6 * uy) * gy);
+  FI[8] = W[2] * rho * (((T)3 + (T)6 * ux - (T)9 * uy) * gx + ((T)-3 - (T)9 * ux + (T)6 * uy) * gy);
+}
+
 // f of edge node (i, j) from the ring of parity par.  FP64: the reference's
 // arithmetic.  FP32 (shifted populations, the ring holding rho - rho0):
 // h_k = W_k (drho B_k + rho0 (B_k - B_k(0))) + rho0 (W_k B_k(0) - w_k), with
@@ -104,24 +144,10 @@ __device__ __forceinline__ void edge_equilibrium(const LatticeArgs& a, int i, in
     for (int k = 0; k < 9; ++k) f[k] = (T)fe[k];
     return;
   }
-  const float x = (float)ux, y = (float)uy, dr = (float)r, r0 = a.m.rho0_f;
-  const float U2 = x * x + y * y;
-  float d[9];  // B_k - B_k(0)
-  d[0] = -3.f * U2;
-  d[1] = 6.f * x + 9.f * x * x - 3.f * U2;
-  d[2] = 6.f * y + 9.f * y * y - 3.f * U2;
-  d[3] = -6.f * x + 9.f * x * x - 3.f * U2;
-  d[4] = -6.f * y + 9.f * y * y - 3.f * U2;
-  d[5] = 3.f * (x + y) + 9.f * x * y + 3.f * U2;
-  d[6] = -3.f * (x - y) - 9.f * x * y + 3.f * U2;
-  d[7] = -3.f * (x + y) + 9.f * x * y + 3.f * U2;
-  d[8] = 3.f * (x - y) - 9.f * x * y + 3.f * U2;
+  float h[9];
+  feq_shift32(a.m, (float)r, (float)ux, (float)uy, h);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const float W = a.m.w_init_f[k == 0 ? 0 : (k < 5 ? 1 : 2)];
-    const float B = (k == 0 || k < 5 ? 2.f : 1.f) + d[k];
-    f[k] = (T)(W * (dr * B + r0 * d[k]) + a.m.eq_c_f[k]);
-  }
+  for (int k = 0; k < 9; ++k) f[k] = (T)h[k];
 }
 
 // ComputeRelaxation_MRT (C1:1029-1048 fixed q; C6:1002-1021 q of omega).
@@ -791,7 +817,94 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
   no.t11 = no.t22 = no.t12 = 0.0;
   const bool want_stress = m.bingham || m.record_stress;
   const bool node_omega = m.bingham && MODE != MODE_INIT;
-  if (F64) {
+  if (m.bgk) {
+    // COLLISION (C1:774-841).  Bingham: the bi-viscosity model on f - FEQ of
+    // the node's previous collision (from its stored density and velocity;
+    // INITIALIZE's equilibrium at the first step, the restored state's own
+    // after a restart), with the node's previous omega.
+    T* pm = static_cast<T*>(a.pm_dst);
+    if (F64) {
+      double om = m.omega;
+      if (m.bingham) {
+        double fp[9];
+        if (MODE == MODE_STEP) {
+          const T* q = static_cast<const T*>(a.pm_src);
+          feq_double(m, (double)q[g.plane + n], (double)q[2 * g.plane + n], (double)q[n], fp);
+        } else if (MODE == MODE_INIT) {
+          feq_double(m, 0.0, 0.0, m.rho0, fp);
+        } else {
+          feq_double(m, (double)uxc, (double)uyc, (double)rho, fp);
+        }
+        const double omp = node_omega ? (double)static_cast<const T*>(a.om_src)[n] : m.omega;
+        const double ZARIB = -1.5 * omp / (double)rho;
+        double F_1[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F_1[k] = (double)f[k] - fp[k];
+        const double D11 = ZARIB * (F_1[1] + F_1[5] + F_1[6] + F_1[3] + F_1[7] + F_1[8]);
+        const double D22 = ZARIB * (F_1[5] + F_1[2] + F_1[6] + F_1[7] + F_1[4] + F_1[8]);
+        const double D12 = ZARIB * (F_1[5] - F_1[6] + F_1[7] - F_1[8]);
+        const double GAMMA = sqrt(4.0 * fabs(D12 * D12 - D11 * D22));
+        double NU_A;
+        if (GAMMA < m.gamma_c) {
+          NU_A = m.mu_r;
+          no.yield = 5;
+        } else {
+          NU_A = m.nu + m.tau_y / GAMMA;
+        }
+        om = 1.0 / (3.0 * NU_A + 0.5);
+        no.omega = om;
+      }
+      double FE[9], FI[9];
+      bgk_source<double>(m.w_src, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, FI);
+      feq_double(m, (double)uxc, (double)uyc, (double)rho, FE);
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        f[k] = (T)(om * FE[k] + (1.0 - om) * (double)f[k] + (1. - 0.5 * om) * FI[k]);
+    } else {
+      float om = m.omega_f;
+      const float dr = (float)drho, rf = (float)rho, xf = (float)uxc, yf = (float)uyc;
+      if (m.bingham) {
+        float hp[9];
+        if (MODE == MODE_STEP) {
+          const T* q = static_cast<const T*>(a.pm_src);
+          feq_shift32(m, (float)q[n], (float)q[g.plane + n], (float)q[2 * g.plane + n], hp);
+        } else if (MODE == MODE_INIT) {
+          feq_shift32(m, 0.0f, 0.0f, 0.0f, hp);
+        } else {
+          feq_shift32(m, dr, xf, yf, hp);
+        }
+        const float omp = node_omega ? (float)static_cast<const T*>(a.om_src)[n] : m.omega_f;
+        const float ZARIB = -1.5f * omp / rf;
+        float F_1[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) F_1[k] = (float)f[k] - hp[k];
+        const float D11 = ZARIB * (F_1[1] + F_1[5] + F_1[6] + F_1[3] + F_1[7] + F_1[8]);
+        const float D22 = ZARIB * (F_1[5] + F_1[2] + F_1[6] + F_1[7] + F_1[4] + F_1[8]);
+        const float D12 = ZARIB * (F_1[5] - F_1[6] + F_1[7] - F_1[8]);
+        const float GAMMA = sqrtf(4.0f * fabsf(D12 * D12 - D11 * D22));
+        float NU_A;
+        if (GAMMA < m.gamma_c_f) {
+          NU_A = m.mu_r_f;
+          no.yield = 5;
+        } else {
+          NU_A = m.nu_f + m.tau_y_f / GAMMA;
+        }
+        om = 1.0f / (3.0f * NU_A + 0.5f);
+        no.omega = om;
+      }
+      float FE[9], FI[9];
+      bgk_source<float>(m.w_src_f, rf, xf, yf, (float)gx, (float)gy, FI);
+      feq_shift32(m, dr, xf, yf, FE);
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        f[k] = (T)(om * FE[k] + (1.0f - om) * (float)f[k] + (1.0f - 0.5f * om) * FI[k]);
+    }
+    if (m.bingham && pm) {
+      pm[n] = F64 ? rho : drho;
+      pm[g.plane + n] = uxc;
+      pm[2 * g.plane + n] = uyc;
+    }
+  } else if (F64) {
     double S[9];
     if (node_omega) {
       rates_double(m, (double)static_cast<const T*>(a.om_src)[n], S);
@@ -1515,6 +1628,8 @@ __global__ void __launch_bounds__(BX * BY)
         s_a.dst = B.f[b ^ 1];
         s_a.om_src = B.om[b];
         s_a.om_dst = B.om[b ^ 1];
+        s_a.pm_src = B.pm[b];
+        s_a.pm_dst = B.pm[b ^ 1];
       }
       __syncthreads();
       qfirst = B.first;
@@ -1543,7 +1658,7 @@ template <class T>
 cudaError_t launch_mode(const LatticeArgs& a, cudaStream_t s, int mode) {
   dim3 grid(a.g.nbx, a.g.nby);
   switch (mode) {
-    case MODE_STEP: return cudaErrorInvalidValue;  // launch_step below
+    case MODE_STEP: k_lattice<T, MODE_STEP><<<grid, TPB, 0, s>>>(a); break;  // BGK steps
     case MODE_OUTPUT: k_lattice<T, MODE_OUTPUT><<<grid, TPB, 0, s>>>(a); break;
     case MODE_INIT: k_lattice<T, MODE_INIT><<<grid, TPB, 0, s>>>(a); break;
     default: k_lattice<T, MODE_RESTART><<<grid, TPB, 0, s>>>(a); break;

@@ -41,6 +41,7 @@ LBM_STRAIN_MEQ, LBM_STRAIN_FEQ = 0, 1
 LBM_NEWTONIAN, LBM_BINGHAM, LBM_CASSON = 0, 1, 2
 LBM_RATES_FIXED_Q, LBM_RATES_Q_OF_OMEGA = 0, 1
 LBM_WALL_MIRROR, LBM_WALL_OFFSET, LBM_WALL_NONE = 0, 1, 2
+LBM_COLLISION_MRT, LBM_COLLISION_BGK = 0, 1
 LBM_CONTACT_DPP, LBM_CONTACT_STALE_DPW = 0, 1
 LBM_PIN, LBM_POUT, LBM_STATE_PER = 8, 16, 20
 LBM_SERIES_HEAD, LBM_SERIES_PER = 2, 12
@@ -113,7 +114,7 @@ class LbmParams(ctypes.Structure):
         ("osc_u", ctypes.c_double),
         ("osc_period", ctypes.c_double),
         ("strain_model", ctypes.c_int32),
-        ("reserved1", ctypes.c_int32),
+        ("collision", ctypes.c_int32),
     ]
 
     def __init__(self, **kw):

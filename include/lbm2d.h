@@ -78,6 +78,16 @@ enum { LBM_STRAIN_MEQ = 0,       /* C6:903-922: m_neq against the moment-space
        LBM_STRAIN_FEQ = 1 };     /* C1:896-948: m_neq against the moments of
                                     COMPUTEFEQNEW, 1/rho folded into both terms */
 
+enum { LBM_COLLISION_MRT = 0,    /* Collision_MRT, C1:875-1048 / C6:867-1021     */
+       LBM_COLLISION_BGK = 1 };  /* COLLISION, C1:774-841: single-relaxation BGK
+                                    with ComputeSourceEquilib_Hydro's forcing
+                                    (C1:843-870); with LBM_BINGHAM its
+                                    bi-viscosity model (C1:789-809): shear rate
+                                    sqrt(4|D12^2 - D11 D22|) from f - FEQ of
+                                    the previous collision, nu = MU_R =
+                                    1000 nu below GAMMA_C = tau_y/(MU_R - nu),
+                                    else nu + tau_y/gamma (C1:51-53)        */
+
 enum { LBM_WALL_MIRROR = 0,     /* C1:737-745: mirror-image wall particles     */
        LBM_WALL_OFFSET = 1,     /* C3:775-783, C6:717-725: wall disk at R out  */
        LBM_WALL_NONE = 2 };
@@ -130,7 +140,7 @@ typedef struct lbm_params {
     double osc_u;             /* U_C of LBM_MOTION_OSCILLATE (C4:30)           */
     double osc_period;        /* T_C of LBM_MOTION_OSCILLATE (C4:32)           */
     int32_t strain_model;     /* LBM_STRAIN_* (non-Newtonian strain rate)      */
-    int32_t reserved1;
+    int32_t collision;        /* LBM_COLLISION_*                               */
 } lbm_params;
 
 /* Particle input record (lbm_set_particles): LBM_PIN doubles per disk. */

@@ -300,6 +300,72 @@ static void collision_mrt(oracle* o) {
         }
 }
 
+/* ---- ComputeSourceEquilib_Hydro, C1:843-870: forcing FI and FEQ with
+ * G_X = G_Y = 0; the forcing weights are the REAL(4) quotients 4.0/9.0,
+ * 1./9., 1./36. ------------------------------------------------------------ */
+static void source_equilib_hydro(const oracle* o, double UX, double UY, double RHO, double GX,
+                                 double GY, double* FI, double* FEQ) {
+    const double W0 = (double)(4.0f / 9.0f), W1 = (double)(1.0f / 9.0f),
+                 W2 = (double)(1.0f / 36.0f);
+    const double gx = GX + 0.0, gy = GY + 0.0;
+    FI[0] = W0 * RHO * (-(3. * UX * gx) - 3. * UY * gy);
+    FI[1] = W1 * RHO * ((3. + 6. * UX) * gx - 3. * UY * gy);
+    FI[2] = W1 * RHO * (-(3. * UX * gx) + (3. + 6. * UY) * gy);
+    FI[3] = W1 * RHO * ((-3. + 6. * UX) * gx - 3. * UY * gy);
+    FI[4] = W1 * RHO * (-(3. * UX * gx) + (-3. + 6. * UY) * gy);
+    FI[5] = W2 * RHO * ((3. + 6. * UX + 9. * UY) * gx + (3. + 9. * UX + 6. * UY) * gy);
+    FI[6] = W2 * RHO * ((-3. + 6. * UX - 9. * UY) * gx + (3. - 9. * UX + 6. * UY) * gy);
+    FI[7] = W2 * RHO * ((-3. + 6. * UX + 9. * UY) * gx + (-3. + 9. * UX + 6. * UY) * gy);
+    FI[8] = W2 * RHO * ((3. + 6. * UX - 9. * UY) * gx + (-3. - 9. * UX + 6. * UY) * gy);
+    compute_feq(o, UX, UY, RHO, FEQ); /* the same expressions as COMPUTEFEQNEW */
+}
+
+/* ---- COLLISION, C1:774-841: BGK; with a Bingham rheology the bi-viscosity
+ * model (C1:789-809) on f - FEQ of the previous call (FEQ holds it until the
+ * node recomputes it), MU_R = 1000 MU_0, GAMMA_C = TAU_Y/(MU_R - MU_0)
+ * (C1:49-53, MU_0 = NU). ---------------------------------------------------- */
+static void collision_bgk(oracle* o) {
+    const int bingham = o->p.rheology == LBM_BINGHAM;
+    const double MU_0 = o->p.nu, MU_R = 1000.0 * MU_0, TAU_Y = o->p.tau_y;
+    const double GAMMA_C = TAU_Y / (MU_R - MU_0);
+    for (int j = 0; j <= o->ny; ++j)
+        for (int i = 0; i <= o->nx; ++i) {
+            size_t n = IDX(o, i, j);
+            double* f = &o->F[Q * n];
+            double* FEQ = &o->FEQ[Q * n];
+            const double RHO = o->RHO[n], UX = o->UX[n], UY = o->UY[n];
+            double om = o->omega;
+            if (bingham) {
+                double ZARIB = -1.5 * o->OMEGA_BN[n] / RHO;
+                double F_1[Q];
+                for (int k = 0; k < Q; ++k) F_1[k] = f[k] - FEQ[k];
+                double D11 = ZARIB * (F_1[1] + F_1[5] + F_1[6] + F_1[3] + F_1[7] + F_1[8]);
+                double D22 = ZARIB * (F_1[5] + F_1[2] + F_1[6] + F_1[7] + F_1[4] + F_1[8]);
+                double D12 = ZARIB * (F_1[5] - F_1[6] + F_1[7] - F_1[8]);
+                double GAMMA = sqrt(4.0 * fabs(D12 * D12 - D11 * D22));
+                double NU_A;
+                if (GAMMA < GAMMA_C) {
+                    NU_A = MU_R;
+                    o->IMAGE[n] = 5;
+                } else {
+                    NU_A = MU_0 + TAU_Y / GAMMA;
+                    o->IMAGE[n] = 0;
+                }
+                o->OMEGA_BN[n] = 1.0 / (3.0 * NU_A + 0.5);
+                om = o->OMEGA_BN[n];
+            }
+            double FI[Q];
+            source_equilib_hydro(o, UX, UY, RHO, o->G[2 * n], o->G[2 * n + 1], FI, FEQ);
+            for (int k = 0; k < Q; ++k)
+                f[k] = om * FEQ[k] + (1.0 - om) * f[k] + (1. - 0.5 * om) * FI[k];
+        }
+}
+
+static void collide(oracle* o) {
+    if (o->p.collision == LBM_COLLISION_BGK) collision_bgk(o);
+    else collision_mrt(o);
+}
+
 /* ---- STREAMING, C1:1181-1217 (pull, out-of-domain sources keep F) ----- */
 static void streaming(oracle* o) {
     for (int j = 0; j <= o->ny; ++j)
@@ -661,7 +727,7 @@ static void one_step(oracle* o) {
         }
     }
     compute_concentration(o);
-    collision_mrt(o);
+    collide(o);
     memcpy(o->FPOST, o->F, Q * o->nn * sizeof(double));
     streaming(o);
     if (o->p.bc == LBM_BC_ZOUHE) bc_zouhe(o);
@@ -843,15 +909,19 @@ int oracle_get_next_post_collision(oracle* o, double* out, double* omega_out) {
     double* Sc = (double*)malloc(3 * o->nn * sizeof(double));
     int32_t* Ic = (int32_t*)malloc(o->nn * sizeof(int32_t));
     if (!Fc || !Oc || !Sc || !Ic) { free(Fc); free(Oc); free(Sc); free(Ic); return LBM_E_NOMEM; }
+    double* FE = o->FEQ;
+    double* FEc = (double*)malloc(Q * o->nn * sizeof(double));
+    if (!FEc) { free(Fc); free(Oc); free(Sc); free(Ic); return LBM_E_NOMEM; }
+    memcpy(FEc, FE, Q * o->nn * sizeof(double));
     memcpy(Fc, F, Q * o->nn * sizeof(double));
     memcpy(Oc, OM, o->nn * sizeof(double));
-    o->F = Fc; o->OMEGA_BN = Oc; o->STRESS = Sc; o->IMAGE = Ic;
-    collision_mrt(o);
+    o->F = Fc; o->OMEGA_BN = Oc; o->STRESS = Sc; o->IMAGE = Ic; o->FEQ = FEc;
+    collide(o);
     memcpy(out, Fc, Q * o->nn * sizeof(double));
     if (omega_out) memcpy(omega_out, Oc, o->nn * sizeof(double));
-    o->F = F; o->OMEGA_BN = OM; o->STRESS = ST; o->IMAGE = IM;
+    o->F = F; o->OMEGA_BN = OM; o->STRESS = ST; o->IMAGE = IM; o->FEQ = FE;
     memcpy(o->omega_mrt, mrt, sizeof mrt);
-    free(Fc); free(Oc); free(Sc); free(Ic);
+    free(Fc); free(Oc); free(Sc); free(Ic); free(FEc);
     return LBM_OK;
 }
 

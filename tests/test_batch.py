@@ -32,6 +32,9 @@ def mixed_cases(cases, precision):
     out.append((p.copy(precision=precision), pin))
     p = cases.shipped_c1(48, 40, 8.0)  # no particles
     out.append((p.copy(precision=precision), None))
+    p = cases.shipped_c1(40, 60, 8.0)  # the BGK collision with the bi-viscosity model
+    p.collision, p.rheology, p.tau_y, p.gravity = 1, 1, 2e-6, -2e-5
+    out.append((p.copy(precision=precision), cases.pin_array([[20.0, 38.0]], 8.0, 1.5)))
     for p, _ in out:
         p.series_every = 5
         p.series_capacity = 4  # the ring fills: the batch drains between chunks

@@ -149,6 +149,62 @@ def test_c3_casson_fp64(pkg, cases):
         close64(sim.field(f), ref.field(f), 1e-8, f)
 
 
+def bgk_case(cases, bingham):
+    """C1 with the BGK COLLISION (C1:774-841) in place of Collision_MRT; with
+    bingham its bi-viscosity model at a yield stress whose threshold
+    GAMMA_C = tau_y/(999 nu) = 4e-8 lies inside the range of shear rates
+    around the disk, so yielded and unyielded nodes both occur (a larger
+    yield stress leaves the whole fluid unyielded at 1000 nu)."""
+    p = cases.shipped_c1(40, 60, 8.0)
+    p.collision = 1  # LBM_COLLISION_BGK
+    p.gravity = -2e-5
+    if bingham:
+        p.rheology = 1  # LBM_BINGHAM: bi-viscosity under BGK
+        p.tau_y = 2e-6
+    pin = cases.pin_array([[20.0, 38.0]], 8.0, 1.5)
+    return p, pin
+
+
+@pytest.mark.parametrize("bingham", [0, 1])
+def test_bgk_collision_fp64(pkg, cases, bingham):
+    """BGK 1e-10; the bi-viscosity switch 1e-8 (as the Papanastasiou path:
+    ulp-level differences of sin and of the force order grow where the
+    viscosity jumps by a factor of 1000), its omega 1e-7 (near GAMMA_C the
+    shear rate comes from f - FEQ differences of ~1e-9 between values of
+    ~0.1, eight digits below the populations)."""
+    p, pin = bgk_case(cases, bingham)
+    sim, ref = pair(pkg, p, pin, 150)
+    om = ref.field("omega")
+    if bingham:
+        assert 0 < np.count_nonzero(om < 0.01) < om.size  # both branches occur
+    tol = 1e-8 if bingham else RTOL64
+    compare_all(sim, ref, rtol=tol)
+    if bingham:
+        close64(sim.field("omega"), om, 1e-7, "omega")
+
+
+@pytest.mark.parametrize("bingham", [0, 1])
+def test_bgk_collision_fp32(pkg, cases, bingham):
+    p, pin = bgk_case(cases, bingham)
+    sim = pkg.Simulation(p.copy(precision=1))
+    sim.set_particles(pin)
+    ref = Oracle(p)
+    ref.set_particles(pin)
+    sim.step(150)
+    ref.step(150)
+    g, r = sim.particles(), ref.particles()
+    close64(g[:, 0:2], r[:, 0:2], 1e-4, "position")
+    close64(g[:, 3:5], r[:, 3:5], 1e-4, "velocity")
+    for f in ("ux", "uy"):
+        close64(sim.field(f), ref.field(f), 1e-4, f)
+    if bingham:
+        # a node at the threshold may take the other branch in FP32: at least
+        # 99 % of the nodes agree, each within 1e-3 of the largest omega
+        a, b = sim.field("omega"), ref.field("omega")
+        agree = np.abs(a - b) <= 1e-3 * np.max(np.abs(b))
+        assert np.mean(agree) >= 0.99, np.mean(agree)
+
+
 @pytest.mark.parametrize("contact", [0, 1])
 def test_multiparticle_fp64(pkg, cases, contact):
     rng = np.random.default_rng(3)

@@ -142,3 +142,19 @@ def test_next_post_collision_matches_next_step(cases):
     assert not np.array_equal(fnext, f_now)
     # mass of the post-collision state = 36*d_mrt * mass of F (C1:911-921)
     assert fnext.sum() == pytest.approx(f_now.sum() * 36.0 * p.d_mrt, rel=1e-14)
+
+
+def test_bgk_biviscosity_first_step(cases):
+    """COLLISION's bi-viscosity model (C1:789-809) on INITIALIZE's state: f
+    equals FEQ everywhere, so the shear rate is zero, every node is
+    unyielded, and OMEGA_BN = 1/(3 MU_R + 0.5) with MU_R = 1000 NU."""
+    from oracle.oracle import Oracle
+
+    p = cases.shipped_c1(12, 16, 4.0)
+    p.collision, p.rheology, p.tau_y = 1, 1, 1e-6
+    o = Oracle(p)
+    o.set_particles(cases.pin_array([[6.0, 9.0]], 4.0, 1.5))
+    o.step(1)
+    om = o.field("omega")
+    assert np.all(om == 1.0 / (3.0 * (1000.0 * p.nu) + 0.5))
+    o.close()
