@@ -396,19 +396,32 @@ int compute_output(lbm_sim* h, bool want_f) {
 }
 
 int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
-  // free old
-  dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
-  dfree(h->series); dfree(h->mass_acc);
-  h->ps = nullptr; h->facc = nullptr; h->nbr = nullptr; h->nbr_count = nullptr;
-  h->nbr_xy = nullptr; h->series = nullptr; h->mass_acc = nullptr;
+  // buffers of the same sizes are kept and cleared, so a driver that resets
+  // its disks between runs pays no allocation
+  const int npad = (std::max(np, 1) + 31) / 32 * 32;
+  const int series_np = std::max(0, std::min(h->p.series_particles, np));
+  const int series_len = LBM_SERIES_HEAD + LBM_SERIES_PER * series_np;
+  const int series_cap = std::max(1, h->p.series_capacity);
+  const bool keep_p = h->ps && npad == h->npad;
+  const bool keep_s = h->series && h->p.series_every > 0 && series_len == h->series_len &&
+                      series_cap == h->series_cap;
+  if (!keep_p) {
+    dfree(h->ps); dfree(h->facc); dfree(h->nbr); dfree(h->nbr_count); dfree(h->nbr_xy);
+    h->ps = nullptr; h->facc = nullptr; h->nbr = nullptr; h->nbr_count = nullptr;
+    h->nbr_xy = nullptr;
+  }
   // records of the old disk set (its record length) are dropped
   series_reset(h, h->kk);
   h->host_series.clear();
   h->host_series_read = 0;
-  if (h->series_pin) cudaFreeHost(h->series_pin);
-  if (h->mass_pin) cudaFreeHost(h->mass_pin);
-  h->series_pin = nullptr;
-  h->mass_pin = nullptr;
+  if (!keep_s) {
+    dfree(h->series); dfree(h->mass_acc);
+    h->series = nullptr; h->mass_acc = nullptr;
+    if (h->series_pin) cudaFreeHost(h->series_pin);
+    if (h->mass_pin) cudaFreeHost(h->mass_pin);
+    h->series_pin = nullptr;
+    h->mass_pin = nullptr;
+  }
   h->np = np;
   h->partials_valid = false;
   // pair search cells cover the Verlet radius D_max + repulsion range + SKIN
@@ -416,33 +429,37 @@ int setup_particle_buffers(lbm_sim* h, int np, double dmax) {
   h->ncx = std::max(1, (int)std::floor((double)h->p.nx / h->cell_size) + 1);
   h->ncy = std::max(1, (int)std::floor((double)h->p.ny / h->cell_size) + 1);
   int rc;
-  h->npad = (std::max(np, 1) + 31) / 32 * 32;
+  h->npad = npad;
   const size_t npa = (size_t)h->npad;
-  if ((rc = dalloc(&h->ps, npa * PS))) return rc;
+  if (!keep_p) {
+    if ((rc = dalloc(&h->ps, npa * PS))) return rc;
+    if ((rc = dalloc(&h->facc, npa * 6))) return rc;
+    if ((rc = dalloc(&h->nbr, npa * MAX_NEIGH))) return rc;
+    if ((rc = dalloc(&h->nbr_count, npa))) return rc;
+    if ((rc = dalloc(&h->nbr_xy, npa * 2))) return rc;
+  }
   CK(cudaMemsetAsync(h->ps, 0, sizeof(double) * npa * PS, h->stream));
-  if ((rc = dalloc(&h->facc, npa * 6))) return rc;
-  if ((rc = dalloc(&h->nbr, npa * MAX_NEIGH))) return rc;
-  if ((rc = dalloc(&h->nbr_count, npa))) return rc;
-  if ((rc = dalloc(&h->nbr_xy, npa * 2))) return rc;
   CK(cudaMemsetAsync(h->facc, 0, sizeof(unsigned long long) * npa * 6, h->stream));
   CK(cudaMemsetAsync(h->nbr_count, 0, sizeof(int) * npa, h->stream));
   CK(cudaMemsetAsync(h->nbr_xy, 0, sizeof(double) * npa * 2, h->stream));
   CK(cudaMemsetAsync(h->tile_count, 0, sizeof(int) * 2 * h->g.ltx * h->g.lty, h->stream));
-  h->series_np = std::max(0, std::min(h->p.series_particles, np));
-  h->series_len = LBM_SERIES_HEAD + LBM_SERIES_PER * h->series_np;
-  h->series_cap = std::max(1, h->p.series_capacity);
+  h->series_np = series_np;
+  h->series_len = series_len;
+  h->series_cap = series_cap;
   if (h->p.series_every > 0) {
-    if ((rc = dalloc(&h->series, (size_t)h->series_cap * h->series_len))) return rc;
-    if ((rc = dalloc(&h->mass_acc, (size_t)h->series_cap))) return rc;
+    if (!keep_s) {
+      if ((rc = dalloc(&h->series, (size_t)h->series_cap * h->series_len))) return rc;
+      if ((rc = dalloc(&h->mass_acc, (size_t)h->series_cap))) return rc;
+      h->series_pcap = 2 * h->series_cap;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&h->series_pin),
+                        sizeof(double) * h->series_pcap * h->series_len, cudaHostAllocDefault) !=
+              cudaSuccess ||
+          cudaHostAlloc(reinterpret_cast<void**>(&h->mass_pin),
+                        sizeof(unsigned long long) * h->series_pcap, cudaHostAllocDefault) !=
+              cudaSuccess)
+        return LBM_E_NOMEM;
+    }
     CK(cudaMemsetAsync(h->mass_acc, 0, sizeof(unsigned long long) * h->series_cap, h->stream));
-    h->series_pcap = 2 * h->series_cap;
-    if (cudaHostAlloc(reinterpret_cast<void**>(&h->series_pin),
-                      sizeof(double) * h->series_pcap * h->series_len, cudaHostAllocDefault) !=
-            cudaSuccess ||
-        cudaHostAlloc(reinterpret_cast<void**>(&h->mass_pin),
-                      sizeof(unsigned long long) * h->series_pcap, cudaHostAllocDefault) !=
-            cudaSuccess)
-      return LBM_E_NOMEM;
   }
   return LBM_OK;
 }
