@@ -800,10 +800,15 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
   }
 
   // ---- mean density at history steps (C1:318): fixed-point, order-free ---
+  // (each node's share rounded to fixed point, as the TMA step kernel does,
+  // so both give the same integer total)
   if (MODE == MODE_STEP && rslot >= 0) {
-    double s0 = warp_sum((double)drho);
+    long long q = !act ? 0
+                  : F64 ? __double2ll_rn((double)drho * MASS_FIX)
+                        : __float2ll_rn((float)drho * (float)MASS_FIX);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
     if (lane == 0) {
-      const long long q = __double2ll_rn(s0 * MASS_FIX);
       if (mass_local) *mass_local += q;
       else atomicAdd(a.mass_acc + rslot, (unsigned long long)q);
     }
@@ -1301,9 +1306,10 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
   const int pt = g.pitch;
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
-  // lane 0: this warp's fixed-point share of the mean-density sum, added to
-  // the history slot once when the warp leaves the loop (integer sums, so
-  // the total is the same as with one atomic per tile)
+  // this thread's fixed-point share of the mean-density sum (rho - rho0 of
+  // each of its nodes times 2^40, rounded once per node), summed over the
+  // warp and added to the history slot once when the warp leaves the loop:
+  // integer sums, so the total does not depend on the order
   long long mass_q = 0;
 
   for (;; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
@@ -1454,10 +1460,9 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
 
     // ---- mean density at history steps (C1:318): fixed-point, order-free -
-    if (rslot >= 0) {
-      const double sd = warp_sum((double)drho);
-      if (lane == 0) mass_q += __double2ll_rn(sd * MASS_FIX);
-    }
+    if (rslot >= 0 && act)
+      mass_q += F64 ? __double2ll_rn((double)drho * MASS_FIX)
+                    : __float2ll_rn((float)drho * (float)MASS_FIX);
     if (!act) continue;
 
     // ---- velocity correction (C1:1138-1152) and collision of the next step
@@ -1518,8 +1523,11 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       rec[3 * P + nd] = (T)no.yield;
     }
   }
-  if (rslot >= 0 && lane == 0 && mass_q != 0)
-    atomicAdd(a.mass_acc + rslot, (unsigned long long)mass_q);
+  if (rslot >= 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mass_q += __shfl_down_sync(0xffffffffu, mass_q, o);
+    if (lane == 0 && mass_q != 0) atomicAdd(a.mass_acc + rslot, (unsigned long long)mass_q);
+  }
 }
 
 // FP32: two CTAs per SM; FP64: one (with 17 warps, one SM sub-partition
