@@ -120,6 +120,9 @@ struct lbm_sim {
   double* adj_g = nullptr;             // [blocks][2]
   int adj_npad = 0;
   bool adj_record = false;  // the particle kernel writes adj_hist (forward pass)
+  cudaStream_t adj_rs = nullptr;  // recompute stream of the reverse sweep
+  // recompute done with slot set 0/1, reverse done with set 0/1, fork/join
+  cudaEvent_t adj_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -644,6 +647,9 @@ void destroy_buffers(lbm_sim* h) {
     dfree(h->adj_w[b]);
   }
   dfree(h->adj_state); dfree(h->adj_p); dfree(h->adj_h); dfree(h->adj_rho); dfree(h->adj_g);
+  for (cudaEvent_t e : h->adj_ev)
+    if (e) cudaEventDestroy(e);
+  if (h->adj_rs) cudaStreamDestroy(h->adj_rs);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -1348,10 +1354,13 @@ const char* lbm_strerror(int code) {
 // Adjoint sweep.  Forward: the time loop from step 0 to n1, keeping every
 // step's particle records and, every L steps, a checkpoint of the state
 // after that step (f*, omega, records, FORCE sums, D_PW).  Reverse, segment
-// by segment from the last: restore the checkpoint into slot 0, recompute
-// the segment forward with the step kernel writing each f*(n), omega(n) into
-// its own slot, then run the level kernels from the segment's last level to
-// its first, each followed by the particle kernel of the step before.
+// by segment from the last: restore the checkpoint into the first slot of
+// the segment's slot set, recompute the segment forward with the step kernel
+// writing each f*(n), omega(n) into its own slot, then run the level kernels
+// from the segment's last level to its first, each followed by the particle
+// kernel of the step before.  Two slot sets: the recompute of a segment runs
+// on a second stream while the level kernels of the segment after it run on
+// the handle's stream, so the two latency-bound kernel chains share the SMs.
 namespace {
 
 size_t adj_slot_bytes(const lbm_sim* h) { return (size_t)10 * h->g.plane * h->esz; }
@@ -1391,6 +1400,10 @@ int adj_reserve(lbm_sim* h, int nslots, int nck, long long nhist) {
         return rc;
     }
     if ((rc = dalloc(&h->adj_g, (size_t)2 * h->g.nbx * h->g.nby))) return rc;
+  }
+  if (!h->adj_rs) {
+    CK(cudaStreamCreateWithFlags(&h->adj_rs, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->adj_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   if (h->adj_npad != h->npad) {
     dfree(h->adj_state); dfree(h->adj_p); dfree(h->adj_h); dfree(h->adj_rho);
@@ -1545,7 +1558,8 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
                                           : std::max<long long>(1, std::llround(std::sqrt((double)N)));
   L = std::max<long long>(1, std::min<long long>(L, std::max<long long>(nlev, 1)));
   const int C = nlev > 0 ? (int)((nlev + L - 1) / L) : 0;
-  int rc = adj_reserve(h, (int)L, C, N + 1);
+  const int nsets = C >= 2 ? 2 : 1;
+  int rc = adj_reserve(h, nsets * (int)L, C, N + 1);
   if (rc) return rc;
   const size_t rec = (size_t)PS * h->npad;
   const size_t sb = adj_slot_bytes(h);
@@ -1590,27 +1604,63 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
   h->p.series_every = 0;
   h->prof = false;
   CK(launch_adj_particles(adj_particle_args(h, obj, N), h->stream));
+  // The recompute stream starts after everything enqueued so far and the
+  // handle's stream ends after everything the recompute stream was given.
+  CK(cudaEventRecord(h->adj_ev[4], h->stream));
+  CK(cudaStreamWaitEvent(h->adj_rs, h->adj_ev[4], 0));
   int ain = 0;
   bool have = false;
-  for (int c = C - 1; c >= 0 && rc == LBM_OK; --c) {
-    const long long t0 = (long long)c * L;
-    const long long hi = std::min<long long>(t0 + L, nlev);
-    CK(cudaMemcpyAsync(h->adj_slots, h->adj_ck + sb * c, sb, cudaMemcpyDeviceToDevice, h->stream));
-    if ((rc = adj_load_small(h, c, t0, ck_partials[c] != 0))) break;
-    for (int s = 0; t0 + 1 + s < hi; ++s)
-      if ((rc = adj_step_slots(h, s))) break;
-    if (rc) break;
-    for (long long n = hi; n >= t0 + 1; --n) {
-      const unsigned char* slot = h->adj_slots + sb * (size_t)(n - t0 - 1);
-      // the first level after a recompute reads the slot the step kernel
-      // just wrote: no early start there
-      CK(adj_level(h, n, slot, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
-                   h->adj_a[ain ^ 1], h->adj_w[ain ^ 1], n == hi ? 0 : 1));
-      have = true;
-      ain ^= 1;
-      CK(launch_adj_particles(adj_particle_args(h, obj, n), h->stream));
+  {
+    struct Join {
+      lbm_sim* h;
+      ~Join() {
+        cudaEventRecord(h->adj_ev[4], h->adj_rs);
+        cudaStreamWaitEvent(h->stream, h->adj_ev[4], 0);
+      }
+    } join{h};
+    // Segment c into slot set c & 1, on the recompute stream (the step and
+    // particle launchers take the handle's stream, switched for the call).
+    auto recompute = [&](int c) -> int {
+      const int set = c & 1;
+      const long long t0 = (long long)c * L;
+      const long long hi = std::min<long long>(t0 + L, nlev);
+      // the level kernels of segment c + 2 are done reading the set
+      CK(cudaStreamWaitEvent(h->adj_rs, h->adj_ev[2 + set], 0));
+      struct Switch {
+        lbm_sim* h;
+        cudaStream_t own;
+        ~Switch() { h->stream = own; }
+      } sw{h, h->stream};
+      h->stream = h->adj_rs;
+      const int base = set * (int)L;
+      CK(cudaMemcpyAsync(h->adj_slots + sb * base, h->adj_ck + sb * c, sb,
+                         cudaMemcpyDeviceToDevice, h->stream));
+      int r = adj_load_small(h, c, t0, ck_partials[c] != 0);
+      for (int s = 0; r == LBM_OK && t0 + 1 + s < hi; ++s) r = adj_step_slots(h, base + s);
+      if (r) return r;
+      CK(cudaEventRecord(h->adj_ev[set], h->stream));
+      return LBM_OK;
+    };
+    if (C > 0) rc = recompute(C - 1);
+    for (int c = C - 1; c >= 0 && rc == LBM_OK; --c) {
+      if (c > 0 && (rc = recompute(c - 1))) break;
+      const int set = c & 1;
+      const long long t0 = (long long)c * L;
+      const long long hi = std::min<long long>(t0 + L, nlev);
+      CK(cudaStreamWaitEvent(h->stream, h->adj_ev[set], 0));
+      for (long long n = hi; n >= t0 + 1; --n) {
+        const unsigned char* slot = h->adj_slots + sb * (size_t)(set * L + n - t0 - 1);
+        // the first level of a segment follows a wait on the recompute
+        // stream: no early start there
+        CK(adj_level(h, n, slot, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
+                     h->adj_a[ain ^ 1], h->adj_w[ain ^ 1], n == hi ? 0 : 1));
+        have = true;
+        ain ^= 1;
+        CK(launch_adj_particles(adj_particle_args(h, obj, n), h->stream));
+      }
+      CK(cudaEventRecord(h->adj_ev[2 + set], h->stream));
     }
-  }
+  }  // the recompute stream joins the handle's stream here
   if (rc) return rc;
   // level 0: the collision of step 1 from INITIALIZE's state (nu, tau_y only)
   CK(adj_level(h, 0, nullptr, have ? h->adj_a[ain] : nullptr, have ? h->adj_w[ain] : nullptr,
@@ -1659,6 +1709,7 @@ struct lbm_batch {
   std::vector<lbm_sim*> sims;
   int device = 0;
   int prec = 0;
+  int bgk = 0;             // some simulation uses the BGK collision
   int nsm = 148;
   cudaStream_t stream = nullptr;
   BatchSim* d_sims = nullptr;
@@ -1719,10 +1770,10 @@ cudaError_t batch_launch_step(lbm_batch* b) {
   cudaError_t e = launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream);
   if (e != cudaSuccess) return e;
   return b->prec == LBM_FP64
-             ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, b->shape, batch_grid(b),
-                                 b->stream)
-             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, b->shape, batch_grid(b),
-                                 b->stream);
+             ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, b->shape, b->bgk,
+                                 batch_grid(b), b->stream)
+             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, b->shape, b->bgk,
+                                 batch_grid(b), b->stream);
 }
 
 // Host bookkeeping of s completed batch steps.
@@ -1761,9 +1812,9 @@ int batch_tune(lbm_batch* b, int32_t& left) {
       CK(launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream));
       CK(cudaEventRecord(b->ev[0], b->stream));
       CK(b->prec == LBM_FP64 ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, sh,
-                                                 batch_grid(b), b->stream)
+                                                 b->bgk, batch_grid(b), b->stream)
                              : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, sh,
-                                                 batch_grid(b), b->stream));
+                                                 b->bgk, batch_grid(b), b->stream));
       CK(cudaEventRecord(b->ev[1], b->stream));
       CK(cudaEventSynchronize(b->ev[1]));
       float ms = 0.f;
@@ -1805,6 +1856,7 @@ int lbm_batch_create(const lbm_params* params, int32_t nsim, lbm_batch** out) {
   };
   b->device = params[0].device;
   b->prec = params[0].precision;
+  for (int q = 0; q < nsim; ++q) b->bgk |= params[q].collision == LBM_COLLISION_BGK;
   for (int q = 0; q < nsim; ++q) {
     lbm_sim* h = nullptr;
     int rc = lbm_create(&params[q], &h);

@@ -16,8 +16,8 @@ cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_RESTART);
 }
 cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, int shape,
-                              int grid, cudaStream_t s) {
-  return launch_batch<float>(sims, nsim, total, shape, grid, s);
+                              int bgk, int grid, cudaStream_t s) {
+  return launch_batch<float>(sims, nsim, total, shape, bgk, grid, s);
 }
 cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_STEP);

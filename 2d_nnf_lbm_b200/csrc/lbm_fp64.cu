@@ -18,8 +18,8 @@ cudaError_t launch_restart_fp64(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<double>(a, s, MODE_RESTART);
 }
 cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
-                              int grid, cudaStream_t s) {
-  return launch_batch<double>(sims, nsim, total, shape, grid, s);
+                              int bgk, int grid, cudaStream_t s) {
+  return launch_batch<double>(sims, nsim, total, shape, bgk, grid, s);
 }
 cudaError_t launch_bgk_step_fp64(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<double>(a, s, MODE_STEP);

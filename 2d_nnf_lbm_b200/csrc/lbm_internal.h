@@ -241,9 +241,9 @@ __host__ __device__ constexpr int batch_bx(int shape) { return shape == 0 ? 32 :
 __host__ __device__ constexpr int batch_by(int shape) { return 256 / batch_bx(shape); }
 
 cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, int shape,
-                              int grid, cudaStream_t s);
+                              int bgk, int grid, cudaStream_t s);
 cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
-                              int grid, cudaStream_t s);
+                              int bgk, int grid, cudaStream_t s);
 cudaError_t prepare_particles_batch();
 cudaError_t launch_particles_batch(const ParticleArgs* args, int nsim, cudaStream_t s);
 

@@ -593,7 +593,9 @@ __device__ __forceinline__ void facc_add(unsigned long long* hi, unsigned long l
 // mass_local (MODE_STEP): when given, lane 0 adds the warp's fixed-point
 // mean-density share there instead of to the history slot (the caller adds
 // the total once); integer sums, so the result is the same.
-template <class T, int MODE, int BX, int BY>
+// BGK: whether the body carries the BGK collision at all (a kernel that only
+// ever sees MRT models leaves it out and keeps its register budget).
+template <class T, int MODE, int BX, int BY, bool BGK = true>
 __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int byi,
                                              long long* mass_local = nullptr) {
   static_assert(LTX % BX == 0 && LTY % BY == 0 && BX % 32 == 0, "tile inside a list tile");
@@ -822,7 +824,7 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
   no.t11 = no.t22 = no.t12 = 0.0;
   const bool want_stress = m.bingham || m.record_stress;
   const bool node_omega = m.bingham && MODE != MODE_INIT;
-  if (m.bgk) {
+  if (BGK && m.bgk) {
     // COLLISION (C1:774-841).  Bingham: the bi-viscosity model on f - FEQ of
     // the node's previous collision (from its stored density and velocity;
     // INITIALIZE's equilibrium at the first step, the restored state's own
@@ -1590,8 +1592,8 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
 // buffers, the step number and the history slot taken from the simulation's
 // device counters (so a captured graph replays unchanged).  The node
 // arithmetic is the scalar step's, so results do not depend on the tile
-// shape or the grid.
-template <class T, int BX, int BY>
+// shape or the grid.  BGK: some simulation of the batch uses the BGK collision.
+template <class T, int BX, int BY, bool BGK>
 __global__ void __launch_bounds__(BX * BY)
     k_lattice_batch(const BatchSim* __restrict__ sims, int nsim, long long total) {
   __shared__ LatticeArgs s_a;
@@ -1646,19 +1648,26 @@ __global__ void __launch_bounds__(BX * BY)
       mass_ptr = (s_a.rec_slot >= 0 && s_a.mass_acc) ? s_a.mass_acc + s_a.rec_slot : nullptr;
     }
     const long long t = item - qfirst;
-    lattice_body<T, MODE_STEP, BX, BY>(s_a, (int)(t % nbx), (int)(t / nbx), &mass_q);
+    lattice_body<T, MODE_STEP, BX, BY, BGK>(s_a, (int)(t % nbx), (int)(t / nbx), &mass_q);
   }
   if ((threadIdx.x & 31) == 0 && mass_ptr && mass_q) atomicAdd(mass_ptr, (unsigned long long)mass_q);
 }
 
-template <class T>
-cudaError_t launch_batch(const BatchSim* sims, int nsim, long long total, int shape, int grid,
-                         cudaStream_t s) {
+template <class T, bool BGK>
+void launch_batch_shape(const BatchSim* sims, int nsim, long long total, int shape, int grid,
+                        cudaStream_t s) {
   switch (shape) {
-    case 0: k_lattice_batch<T, 32, 8><<<grid, 256, 0, s>>>(sims, nsim, total); break;
-    case 1: k_lattice_batch<T, 64, 4><<<grid, 256, 0, s>>>(sims, nsim, total); break;
-    default: k_lattice_batch<T, 128, 2><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+    case 0: k_lattice_batch<T, 32, 8, BGK><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+    case 1: k_lattice_batch<T, 64, 4, BGK><<<grid, 256, 0, s>>>(sims, nsim, total); break;
+    default: k_lattice_batch<T, 128, 2, BGK><<<grid, 256, 0, s>>>(sims, nsim, total); break;
   }
+}
+
+template <class T>
+cudaError_t launch_batch(const BatchSim* sims, int nsim, long long total, int shape, int bgk,
+                         int grid, cudaStream_t s) {
+  if (bgk) launch_batch_shape<T, true>(sims, nsim, total, shape, grid, s);
+  else launch_batch_shape<T, false>(sims, nsim, total, shape, grid, s);
   return cudaGetLastError();
 }
 
