@@ -1728,7 +1728,7 @@ struct lbm_batch {
 namespace {
 
 constexpr int BATCH_GRAPH_STEPS = 8;
-constexpr int BATCH_BPSM[3] = {2, 4, 8};
+constexpr int BATCH_BPSM[3] = {2, 4, 6};
 
 int batch_grid(const lbm_batch* b) {
   const long long g = (long long)b->bpsm * b->nsm;

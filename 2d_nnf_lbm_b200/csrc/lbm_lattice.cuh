@@ -1593,8 +1593,15 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
 // device counters (so a captured graph replays unchanged).  The node
 // arithmetic is the scalar step's, so results do not depend on the tile
 // shape or the grid.  BGK: some simulation of the batch uses the BGK collision.
+// FP32 MRT: six blocks per SM (40 registers, a few spilled) hide more of the
+// gather latency than four at 64 registers; the BGK variant keeps four
+// (its larger body would spill much more at 40); FP64 takes the compiler's
+// register count.
+#ifndef LBM_BATCH_MINB_F32
+#define LBM_BATCH_MINB_F32 6
+#endif
 template <class T, int BX, int BY, bool BGK>
-__global__ void __launch_bounds__(BX * BY)
+__global__ void __launch_bounds__(BX * BY, sizeof(T) == 8 ? 0 : (BGK ? 4 : LBM_BATCH_MINB_F32))
     k_lattice_batch(const BatchSim* __restrict__ sims, int nsim, long long total) {
   __shared__ LatticeArgs s_a;
   __shared__ int s_sim;

@@ -12,7 +12,7 @@ kernel launches without the timing harness around them:
              with the objective window over the last 100 steps
   --batch N  the first N runs of the batched workload (Bingham single-disk
              runs of widths 128..512), lbm_batch_step with 32 x 8 tiles and
-             4 blocks per SM
+             6 blocks per SM
 Prints the step count, the first disk's centre (or J and its gradient) and
 the device status.
 """
@@ -50,7 +50,7 @@ def main(argv=None) -> int:
     if a.batch > 0:
         cs = pkg.cases.workload_cfg4(prec)[: a.batch]
         b = pkg.Batch([q for q, _ in cs])
-        b.set_tuning(32, 8, 4)
+        b.set_tuning(32, 8, 6)
         for s, (_, disks) in zip(b.sims, cs):
             s.set_particles(disks)
         b.step(a.steps)
