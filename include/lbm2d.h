@@ -274,6 +274,11 @@ const char* lbm_strerror(int code);
  * checkpoints every `checkpoint_every` steps (0: round(sqrt(n1))), each
  * segment recomputed forward and its states reversed through the transposed
  * collision / streaming / boundary / SPM / force / Newton-Euler steps.
+ * Device memory kept by the handle: ceil((n1 - 1) / L) checkpoints, two sets
+ * of L slots (one set when there is a single segment), each 10 lattice
+ * planes, L = checkpoint_every; a segment's recompute runs on a second
+ * stream of the handle beside the reverse sweep of the segment after it.
+ * The call returns when the sweep is done.
  * grads receives 2 + 3*np doubles:
  *   [LBM_GRAD_TAU_Y] dJ/dtau_y   [LBM_GRAD_NU] dJ/dnu (plastic viscosity)
  *   then per disk p: dJ/drho_p, dJ/dx0, dJ/dy0 at LBM_GRAD_HEAD + 3p.
