@@ -588,6 +588,13 @@ __device__ __forceinline__ void facc_add(unsigned long long* hi, unsigned long l
 #define LBM_MINB_F64 1
 #endif
 
+// FP32 node share of the mean-density sum in units of 2^-40: drho rounded to
+// a multiple of 2^-30 by a 32-bit conversion (|drho| < 2; beyond that it
+// saturates), then widened, which is cheaper than a 64-bit conversion.
+__device__ __forceinline__ long long mass_share32(float drho) {
+  return (long long)__float2int_rn(drho * 0x1p30f) * 1024;
+}
+
 // One tile of BX x BY nodes (block (bxi, byi) of the lattice), one node per
 // thread; BX*BY threads.  The tile lies inside one LTX x LTY list tile.
 // mass_local (MODE_STEP): when given, lane 0 adds the warp's fixed-point
@@ -807,7 +814,7 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
   if (MODE == MODE_STEP && rslot >= 0) {
     long long q = !act ? 0
                   : F64 ? __double2ll_rn((double)drho * MASS_FIX)
-                        : __float2ll_rn((float)drho * (float)MASS_FIX);
+                        : mass_share32((float)drho);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
     if (lane == 0) {
@@ -1309,7 +1316,8 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
   // this thread's fixed-point share of the mean-density sum (rho - rho0 of
-  // each of its nodes times 2^40, rounded once per node), summed over the
+  // each of its nodes in units of 2^-40, rounded once per node: FP64 at
+  // 2^-40, FP32 at 2^-30 by mass_share32), summed over the
   // warp and added to the history slot once when the warp leaves the loop:
   // integer sums, so the total does not depend on the order
   long long mass_q = 0;
@@ -1464,7 +1472,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // ---- mean density at history steps (C1:318): fixed-point, order-free -
     if (rslot >= 0 && act)
       mass_q += F64 ? __double2ll_rn((double)drho * MASS_FIX)
-                    : __float2ll_rn((float)drho * (float)MASS_FIX);
+                    : mass_share32((float)drho);
     if (!act) continue;
 
     // ---- velocity correction (C1:1138-1152) and collision of the next step
