@@ -1330,6 +1330,14 @@ int lbm_get_status(lbm_sim* h) {
   return sticky_status(h);
 }
 
+int lbm_selftest_wait(lbm_sim* h, int32_t limit) {
+  if (!h || limit < 1 || limit > (1 << 20)) return LBM_E_INVALID;
+  cudaSetDevice(h->p.device);
+  CK(launch_wait_selftest(h->d_status, (uint32_t)limit, h->stream));
+  CK(d2h(h, h->h_status, h->d_status, sizeof(int)));
+  return LBM_OK;
+}
+
 const char* lbm_strerror(int code) {
   switch (code) {
     case LBM_OK: return "ok";

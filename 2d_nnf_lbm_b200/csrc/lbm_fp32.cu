@@ -19,6 +19,23 @@ cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, i
                               int bgk, int grid, cudaStream_t s) {
   return launch_batch<float>(sims, nsim, total, shape, bgk, grid, s);
 }
+// The failure path of the bounded wait: one thread waits on a fresh
+// mbarrier that nothing arrives at (phase 0 never completes), gives up after
+// `limit` polls and flags the timeout as the step kernel does.
+__global__ void k_wait_selftest(int* status, uint32_t limit) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(&bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (!mbar_wait(b, 0, limit)) atomicOr(status, ST_TIMEOUT);
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(b) : "memory");
+}
+
+cudaError_t launch_wait_selftest(int* status, uint32_t limit, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(status, limit);
+  return cudaGetLastError();
+}
 cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_STEP);
 }

@@ -245,6 +245,7 @@ cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, i
 cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
                               int bgk, int grid, cudaStream_t s);
 cudaError_t prepare_particles_batch();
+cudaError_t launch_wait_selftest(int* status, uint32_t limit, cudaStream_t s);
 cudaError_t launch_particles_batch(const ParticleArgs* args, int nsim, cudaStream_t s);
 
 // ---------------------------------------------------------------------------

@@ -265,6 +265,7 @@ def load_library():
         "lbm_get_state": ([vp, dp, dp, dp], ctypes.c_int),
         "lbm_set_state": ([vp, ctypes.c_int64, dp, dp, ctypes.c_int32, dp], ctypes.c_int),
         "lbm_get_status": ([vp], ctypes.c_int),
+        "lbm_selftest_wait": ([vp, ctypes.c_int32], ctypes.c_int),
         "lbm_get_stream": ([vp, P(vp)], ctypes.c_int),
         "lbm_profile": ([vp, ctypes.c_int32], ctypes.c_int),
         "lbm_profile_read": ([vp, dp, P(ctypes.c_int64)], ctypes.c_int),
@@ -429,6 +430,11 @@ class Simulation:
 
     def status(self) -> int:
         return int(self.lib.lbm_get_status(self._h))
+
+    def selftest_wait(self, limit: int = 1024) -> None:
+        """Run one bounded device wait that cannot complete (the failure path
+        of the kernels' waits); afterwards status() is LBM_E_TIMEOUT."""
+        self._check(self.lib.lbm_selftest_wait(self._h, int(limit)), "lbm_selftest_wait")
 
     def stream(self) -> int:
         """The handle's cudaStream_t as an integer (for external events)."""

@@ -248,6 +248,15 @@ int lbm_set_state(lbm_sim* h, int64_t kk, const double* f, const double* omega,
 /* Sticky device status (NaN, overflow, timeout); 0 when healthy. */
 int lbm_get_status(lbm_sim* h);
 
+/* Check of the failure path of the kernels' bounded waits (no counterpart in
+ * the reference): on the handle's stream, one thread waits on a fresh
+ * mbarrier that nothing arrives at, with the same bounded wait the step
+ * kernel uses, and gives up after `limit` polls (1..1048576), setting the
+ * handle's timeout status as a step kernel whose wait expired does.  The
+ * handle then reports LBM_E_TIMEOUT from lbm_get_status and refuses further
+ * steps (sticky); the device and other handles are unaffected. */
+int lbm_selftest_wait(lbm_sim* h, int32_t limit);
+
 /* The handle's CUDA stream (a cudaStream_t), so a caller can order its own
  * work or record events against the library's kernels.  The reference has
  * no counterpart (it is single-threaded host code). */
