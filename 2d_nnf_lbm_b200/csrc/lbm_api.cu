@@ -79,7 +79,8 @@ struct lbm_sim {
   std::vector<double> host_series;
   size_t host_series_read = 0;
   // pinned staging ring of the history records and their mean-density sums,
-  // filled by copies queued on the stream after the kernels that wrote them
+  // filled by copies on copy_stream queued after the kernels that wrote them
+  // (so the next steps' kernels run while they cross to the host)
   double* series_pin = nullptr;              // [series_pcap][series_len]
   unsigned long long* mass_pin = nullptr;    // [series_pcap]
   int series_pcap = 0;
@@ -89,6 +90,9 @@ struct lbm_sim {
   };
   std::deque<SeriesBatch> series_pending;
   std::vector<cudaEvent_t> series_ev_free;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_fork = nullptr;  // the kernels that wrote a batch, on stream
+  int64_t ring_free = 0;  // the stream has waited for the copies of records < ring_free
   // COMPUTEERROR: velocity of the previous call, per-block partial sums
   double* u0 = nullptr;       // [2][nodes]
   double* err_part = nullptr;
@@ -301,11 +305,14 @@ cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
 }
 
 // History records.  Record r (step (r+1)*every) sits in slot r % series_cap
-// of the device ring.  series_enqueue queues, on the handle's stream after
-// the kernels that wrote them, the copies of the records not yet queued into
-// the pinned staging ring (slot r % series_pcap), with their mean-density
-// sums, and clears those sums on the device; series_absorb_one waits for the
-// oldest queued batch only and moves it into host_series.
+// of the device ring.  series_enqueue queues, on the copy stream after the
+// kernels that wrote them (an event of the handle's stream), the copies of
+// the records not yet queued into the pinned staging ring (slot
+// r % series_pcap), with their mean-density sums, and clears those sums on
+// the device; before a step writes a slot again, ring_wait makes the
+// handle's stream wait for the copy of the slot's previous record.
+// series_absorb_one waits for the oldest queued batch only and moves it into
+// host_series.
 int series_absorb_one(lbm_sim* h) {
   const lbm_sim::SeriesBatch b = h->series_pending.front();
   CK(cudaEventSynchronize(b.ev));
@@ -341,15 +348,17 @@ int series_enqueue(lbm_sim* h) {
     if ((rc = series_absorb_one(h))) return rc;
   const size_t len = (size_t)h->series_len;
   const long long cap = h->series_cap, pcap = h->series_pcap;
+  CK(cudaEventRecord(h->copy_fork, h->stream));
+  CK(cudaStreamWaitEvent(h->copy_stream, h->copy_fork, 0));
   for (long long r = r0; r < r1;) {
     const long long ds = r % cap, ps = r % pcap;
     const long long cnt = std::min(r1 - r, std::min(cap - ds, pcap - ps));
     CK(cudaMemcpyAsync(h->series_pin + ps * len, h->series + ds * len, cnt * len * sizeof(double),
-                       cudaMemcpyDeviceToHost, h->stream));
+                       cudaMemcpyDeviceToHost, h->copy_stream));
     CK(cudaMemcpyAsync(h->mass_pin + ps, h->mass_acc + ds, cnt * sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, h->stream));
+                       cudaMemcpyDeviceToHost, h->copy_stream));
     // the slots start at zero again before the ring comes back to them
-    CK(cudaMemsetAsync(h->mass_acc + ds, 0, cnt * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->mass_acc + ds, 0, cnt * sizeof(unsigned long long), h->copy_stream));
     r += cnt;
   }
   cudaEvent_t ev = nullptr;
@@ -359,7 +368,7 @@ int series_enqueue(lbm_sim* h) {
   } else {
     CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   }
-  CK(cudaEventRecord(ev, h->stream));
+  CK(cudaEventRecord(ev, h->copy_stream));
   h->series_pending.push_back({r1, ev});
   h->copied_kk = r1 * every;
   return LBM_OK;
@@ -374,12 +383,37 @@ int drain_series(lbm_sim* h) {
   return LBM_OK;
 }
 
-// Drop the queued batches (their copies have completed: callers synchronise
-// the stream first) and the records not yet drained.
+// Drop the queued batches (callers synchronise the handle's stream first;
+// the copies are waited for here) and the records not yet drained.
 void series_reset(lbm_sim* h, long long kk) {
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for (const auto& b : h->series_pending) h->series_ev_free.push_back(b.ev);
   h->series_pending.clear();
   h->drained_kk = h->copied_kk = kk;
+  h->ring_free = h->p.series_every > 0 ? kk / h->p.series_every + h->series_cap : 0;
+}
+
+// Before the step that writes record r: the handle's stream waits for the
+// copy (and the cleared sum) of the record that held its slot before,
+// r - series_cap, unless it has already waited for it or the host has seen
+// that copy complete.
+int ring_wait(lbm_sim* h, long long r) {
+  const long long prev = r - h->series_cap;
+  if (prev < 0 || r < h->ring_free) return LBM_OK;
+  const long long drained = h->drained_kk / h->p.series_every;
+  if (prev < drained) {  // absorbed: its copy has completed
+    h->ring_free = drained + h->series_cap;
+    return LBM_OK;
+  }
+  // queued (enqueue_step queues a record's copy before its slot comes back)
+  for (const auto& b : h->series_pending) {
+    if (b.r_end > prev) {
+      CK(cudaStreamWaitEvent(h->stream, b.ev, 0));
+      h->ring_free = b.r_end + h->series_cap;
+      return LBM_OK;
+    }
+  }
+  return LBM_E_STATE;
 }
 
 // Fields of step kk in h->out (and F after BC in h->out_f when want_f).
@@ -651,6 +685,11 @@ void destroy_buffers(lbm_sim* h) {
     if (e) cudaEventDestroy(e);
   if (h->adj_rs) cudaStreamDestroy(h->adj_rs);
   if (h->h_status) cudaFreeHost(h->h_status);
+  if (h->copy_stream) {
+    cudaStreamSynchronize(h->copy_stream);
+    cudaStreamDestroy(h->copy_stream);
+  }
+  if (h->copy_fork) cudaEventDestroy(h->copy_fork);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -692,7 +731,11 @@ __global__ void __launch_bounds__(ERR_TPB) k_error(const double* ux, const doubl
 int enqueue_step(lbm_sim* h) {
   const int every = h->p.series_every;
   if (h->series && every > 0 && (h->kk + 1) / every - h->copied_kk / every > h->series_cap) {
-    int rc = series_enqueue(h);  // stream-ordered: the ring slots are copied before reuse
+    int rc = series_enqueue(h);  // the ring slots are copied before reuse
+    if (rc) return rc;
+  }
+  if (h->series && every > 0 && (h->kk + 1) % every == 0) {
+    int rc = ring_wait(h, (h->kk + 1) / every - 1);
     if (rc) return rc;
   }
   if (h->prof) {
@@ -909,7 +952,9 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
     delete h;
     return code;
   };
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->copy_fork, cudaEventDisableTiming) != cudaSuccess)
     return fail(LBM_E_CUDA);
   if (cudaHostAlloc(reinterpret_cast<void**>(&h->h_status), sizeof(int), cudaHostAllocDefault) !=
       cudaSuccess)
