@@ -214,10 +214,10 @@ int lbm_get_image(lbm_sim* h, int32_t* out);
 
 /* Drain up to max_records history records into out, oldest first; *nrec =
  * number copied.  Record length is lbm_series_record_len(h) doubles.  Each
- * lbm_step call queues the copies of its records behind its kernels; this
- * call waits only for the copies of the records it returns, so steps queued
- * later keep running while the caller reads them.  The status returned is
- * that of the last completed lbm_step. */
+ * lbm_step call queues the copies of its records after its kernels, on a
+ * second stream of the handle, so the steps queued next run while they
+ * cross to the host; this call waits only for the copies of the records it
+ * returns.  The status returned is that of the last completed lbm_step. */
 int lbm_get_series(lbm_sim* h, double* out, int32_t max_records, int32_t* nrec);
 int lbm_series_record_len(lbm_sim* h, int32_t* len);
 
