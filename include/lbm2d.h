@@ -258,8 +258,10 @@ int lbm_get_status(lbm_sim* h);
 int lbm_selftest_wait(lbm_sim* h, int32_t limit);
 
 /* The handle's CUDA stream (a cudaStream_t), so a caller can order its own
- * work or record events against the library's kernels.  The reference has
- * no counterpart (it is single-threaded host code). */
+ * work or record events against the library's kernels.  The copies of the
+ * history records run on a second, internal stream; lbm_get_series is the
+ * way to wait for them.  The reference has no counterpart (it is
+ * single-threaded host code). */
 int lbm_get_stream(lbm_sim* h, void** stream);
 
 /* Per-kernel device timing, for profiling the time loop (the reference only
