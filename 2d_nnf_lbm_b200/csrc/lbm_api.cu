@@ -556,9 +556,45 @@ int write_particles(lbm_sim* h, const std::vector<double>& buf) {
   std::vector<double> soa(npad * PS, 0.0);
   for (int i = 0; i < h->np; ++i)
     for (int f = 0; f < PS; ++f) soa[(size_t)f * npad + i] = buf[(size_t)i * PS + f];
+  // from pageable memory: the call returns once soa has been staged, so the
+  // vector may go out of scope without a stream synchronisation
   CK(h2d(h, h->ps, soa.data(), soa.size() * sizeof(double)));
-  CK(cudaStreamSynchronize(h->stream));
   return LBM_OK;
+}
+
+// Whether two input disks overlap (centre distance below the sum of the
+// radii), by a cell grid of the largest diameter: O(np) on the host.
+bool disks_overlap(const double* pin, int np, double dmax) {
+  if (np < 2 || !(dmax > 0.0)) return false;
+  const double cs = dmax;
+  std::vector<std::pair<long long, int>> key((size_t)np);
+  for (int i = 0; i < np; ++i) {
+    const double* r = pin + (size_t)LBM_PIN * i;
+    const long long cx = (long long)std::floor(r[0] / cs), cy = (long long)std::floor(r[1] / cs);
+    key[(size_t)i] = {cy * 1000003LL + cx, i};
+  }
+  std::sort(key.begin(), key.end());
+  auto cell_range = [&](long long k) {
+    auto lo = std::lower_bound(key.begin(), key.end(), std::make_pair(k, -1));
+    auto hi = std::lower_bound(key.begin(), key.end(), std::make_pair(k + 1, -1));
+    return std::make_pair(lo, hi);
+  };
+  for (int i = 0; i < np; ++i) {
+    const double* a = pin + (size_t)LBM_PIN * i;
+    const long long cx = (long long)std::floor(a[0] / cs), cy = (long long)std::floor(a[1] / cs);
+    for (long long dy = -1; dy <= 1; ++dy)
+      for (long long dx = -1; dx <= 1; ++dx) {
+        const auto rg = cell_range((cy + dy) * 1000003LL + cx + dx);
+        for (auto it = rg.first; it != rg.second; ++it) {
+          const int j = it->second;
+          if (j <= i) continue;
+          const double* b = pin + (size_t)LBM_PIN * j;
+          const double ex = a[0] - b[0], ey = a[1] - b[1], rs = 0.5 * (a[6] + b[6]);
+          if (ex * ex + ey * ey < rs * rs) return true;
+        }
+      }
+  }
+  return false;
 }
 
 template <class T>
@@ -654,6 +690,10 @@ int make_tensor_maps(lbm_sim* h) {
 }
 
 void destroy_buffers(lbm_sim* h) {
+  // history copies still in flight on the copy stream read the device ring
+  // and write the pinned staging ring: let them finish before anything goes
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  if (h->adj_rs) cudaStreamSynchronize(h->adj_rs);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->ev.clear();
   for (int b = 0; b < 2; ++b) {
@@ -685,10 +725,7 @@ void destroy_buffers(lbm_sim* h) {
     if (e) cudaEventDestroy(e);
   if (h->adj_rs) cudaStreamDestroy(h->adj_rs);
   if (h->h_status) cudaFreeHost(h->h_status);
-  if (h->copy_stream) {
-    cudaStreamSynchronize(h->copy_stream);
-    cudaStreamDestroy(h->copy_stream);
-  }
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->copy_fork) cudaEventDestroy(h->copy_fork);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -1043,6 +1080,10 @@ int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
     if (r[0] < 0.0 || r[0] > h->p.nx || r[1] < 0.0 || r[1] > h->p.ny) return LBM_E_PARTICLE;
     dmax = std::max(dmax, r[6]);
   }
+  // overlapping input disks (no reference input holds any; the repulsion
+  // model's contact branch is for disks that come into contact while moving)
+  if (disks_overlap(pin, np, dmax)) return LBM_E_PARTICLE;
+  // kernels still in flight may read the particle buffers reused below
   CK(cudaStreamSynchronize(h->stream));
   int rc = setup_particle_buffers(h, np, dmax);
   if (rc) return rc;
@@ -1053,7 +1094,6 @@ int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
   }
   if ((rc = write_particles(h, buf))) return rc;
   if ((rc = launch_tiles(h))) return rc;
-  CK(cudaStreamSynchronize(h->stream));
   h->out_kk = -1;
   series_reset(h, h->kk);
   return refreshed_status(h);
@@ -1392,7 +1432,9 @@ const char* lbm_strerror(int code) {
     case LBM_E_CUDA: return "CUDA error (no device or launch failure)";
     case LBM_E_NAN: return "non-finite density or particle state";
     case LBM_E_TIMEOUT: return "bounded device wait expired";
-    case LBM_E_OVERFLOW: return "too many particles touch one lattice tile";
+    case LBM_E_OVERFLOW:
+      return "fixed capacity exceeded (particles per lattice tile or neighbours per particle, "
+             "or an FP32 density deviation of 2 or more)";
     case LBM_E_STATE: return "call out of order";
     case LBM_E_PARTICLE: return "particle outside the lattice";
     case LBM_E_ABI: return "lbm_params.struct_size mismatch";

@@ -595,6 +595,20 @@ __device__ __forceinline__ long long mass_share32(float drho) {
   return (long long)__float2int_rn(drho * 0x1p30f) * 1024;
 }
 
+// Lattice health, once per warp and tile: a node whose density is not
+// finite (a blow-up anywhere in the fluid, with or without disks nearby)
+// sets ST_NAN; in FP32 a finite |rho - rho0| >= 2, beyond the range of
+// mass_share32, sets ST_OVERFLOW.  Every lane of the warp calls it; nodes
+// outside the lattice pass drho = 0.
+template <class T>
+__device__ __forceinline__ void lattice_health(int* status, T drho, int lane) {
+  const bool bad = sizeof(T) == 8 ? !isfinite((double)drho) : !(fabsf((float)drho) < 2.0f);
+  if (__any_sync(0xffffffffu, bad)) {
+    const bool nf = __any_sync(0xffffffffu, !isfinite((double)drho));
+    if (lane == 0) atomicOr(status, nf ? ST_NAN : ST_OVERFLOW);
+  }
+}
+
 // One tile of BX x BY nodes (block (bxi, byi) of the lattice), one node per
 // thread; BX*BY threads.  The tile lies inside one LTX x LTY list tile.
 // mass_local (MODE_STEP): when given, lane 0 adds the warp's fixed-point
@@ -734,6 +748,7 @@ __device__ __forceinline__ void lattice_body(const LatticeArgs& a, int bxi, int 
     drho = (T)0;
     ux = uy = (T)0;
   }
+  if (MODE == MODE_STEP) lattice_health<T>(a.status, drho, lane);
 
   // ---- SPM: G (last particle with PHI>0 wins) and the hydrodynamic force -
   T gx = (T)0, gy = (T)0;
@@ -1390,6 +1405,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       drho = (T)0;
       ux = uy = (T)0;
     }
+    lattice_health<T>(a.status, drho, lane);
     // FP64 reads f back from the stage after the particle loop instead of
     // holding 18 registers across it; edge nodes park theirs there first
     if (F64 && edge && act) {

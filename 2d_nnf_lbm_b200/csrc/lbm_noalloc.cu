@@ -24,6 +24,7 @@
 // variables, C1:464-480 solid fraction and image, C1:488-507 body force with
 // the last particle winning, C1:1138-1152 velocity correction), compiled with
 // --fmad=false like the other FP64 translation units.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -44,18 +45,55 @@ struct NaScratch {
   int count[NA_MAX_TILES];
   int list[NA_MAX_TILES * NA_CAP];
   int overflow;
+  int nonfinite;
 };
 
 static __device__ __align__(256) NaScratch na_scratch;
 
-// Device address of na_scratch, looked up once per device.
+// Device address of na_scratch, looked up once per device and context: the
+// cache holds the driver's unique id of the context the address belongs to,
+// so after a cudaDeviceReset (a new primary context, the module loaded
+// again) the next call looks the address up again instead of using a
+// dangling one.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
 std::mutex na_mutex;
-NaScratch* na_ptr[64] = {};
+struct NaCache {
+  NaScratch* ptr;
+  unsigned long long ctx_id;
+};
+NaCache na_cache[64] = {};
+CtxGetCurrentFn na_ctx_current = nullptr;
+CtxGetIdFn na_ctx_id = nullptr;
+
+// The id of the calling thread's current context (0 when none is current
+// or the driver lacks cuCtxGetId).
+unsigned long long current_ctx_id() {
+  if (!na_ctx_current || !na_ctx_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return 0;
+    na_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    na_ctx_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (na_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (na_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 __global__ void k_na_clear(NaScratch* s, int ntiles) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x)
     s->count[t] = 0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) s->overflow = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s->overflow = 0;
+    s->nonfinite = 0;
+  }
 }
 
 // Disk p into the lists of every list tile within R + zeta/2 + 1 of its
@@ -66,7 +104,11 @@ __global__ void k_na_insert(NaScratch* s, const double* pin, int np, int nx, int
   if (p >= np) return;
   const double* r = pin + (long long)p * LBM_PIN;
   const double x = r[0], y = r[1], rad = 0.5 * r[6] + 0.5 * zeta + 1.0;
-  if (!isfinite(x) || !isfinite(y) || !isfinite(rad)) return;
+  if (!isfinite(x) || !isfinite(y) || !isfinite(rad) || !isfinite(r[3]) || !isfinite(r[4]) ||
+      !isfinite(r[5])) {
+    atomicExch(&s->nonfinite, 1);  // reported as LBM_E_NAN; the disk is left out
+    return;
+  }
   const int i0 = max((int)ceil(x - rad), 0), i1 = min((int)floor(x + rad), nx);
   const int j0 = max((int)ceil(y - rad), 0), j1 = min((int)floor(y + rad), ny);
   if (i0 > i1 || j0 > j1) return;
@@ -159,18 +201,24 @@ extern "C" int lbm_fields_noalloc(const lbm_params* p, const double* f, int32_t 
   if ((long long)ltx * lty > NA_MAX_TILES || np > NA_MAX_PARTICLES) return LBM_E_SCRATCH;
   const int ntiles = ltx * lty;
 
-  // Set-up, once per device: the device address of the static scratch.
+  // Set-up, once per device (and again after the device's context was
+  // replaced): the device address of the static scratch, with that device
+  // current.  The first call on a device does this, so it should come
+  // before any stream capture.
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LBM_E_CUDA;
   NaScratch* s = nullptr;
   {
     std::lock_guard<std::mutex> lock(na_mutex);
-    if (!na_ptr[dev]) {
+    unsigned long long id = current_ctx_id();
+    if (!na_cache[dev].ptr || id == 0 || id != na_cache[dev].ctx_id) {
       void* ptr = nullptr;
       if (cudaGetSymbolAddress(&ptr, na_scratch) != cudaSuccess || !ptr) return LBM_E_CUDA;
-      na_ptr[dev] = static_cast<NaScratch*>(ptr);
+      na_cache[dev].ptr = static_cast<NaScratch*>(ptr);
+      // the runtime has made the device's context current by now
+      na_cache[dev].ctx_id = id ? id : current_ctx_id();
     }
-    s = na_ptr[dev];
+    s = na_cache[dev].ptr;
   }
 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -181,11 +229,12 @@ extern "C" int lbm_fields_noalloc(const lbm_params* p, const double* f, int32_t 
   k_na_fields<<<grid, 256, 0, st>>>(s, f, particles, out, p->nx, p->ny, ltx, p->zeta, p->pi);
   if (cudaGetLastError() != cudaSuccess) return LBM_E_CUDA;
 
-  // The overflow flag decides the return code: wait for this call's work.
-  int overflow = 0;
-  if (cudaMemcpyAsync(&overflow, &s->overflow, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+  // The flags decide the return code: wait for this call's work.
+  int flags[2] = {0, 0};
+  if (cudaMemcpyAsync(flags, &s->overflow, sizeof(flags), cudaMemcpyDeviceToHost, st) !=
           cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return LBM_E_CUDA;
-  return overflow ? LBM_E_OVERFLOW : LBM_OK;
+  if (flags[1]) return LBM_E_NAN;
+  return flags[0] ? LBM_E_OVERFLOW : LBM_OK;
 }

@@ -17,14 +17,24 @@ Arms:
                      its loop structure (the Fortran itself cannot be built
                      in this image), single-threaded as the reference is
 
-Adjoint (N=1): the "adjoint" object times lbm_adjoint on the adjoint
-workload (400x1200, one Bingham disk, 4000 steps, sqrt(N) checkpoints)
-against the forward time loop and checks its FP32 gradient against FP64
-central differences; --no-adjoint skips it.
+Objects of the JSON line beside the headline (N=1; --parts selects them):
+  trajectory_err  FP32 against FP64 on the bench workload over the
+                  multi-particle configuration's 50,000 steps
+  viscoplastic    the viscoplastic-settling workload (800x2400, one Bingham
+                  disk D=40, Bn in {0.5, 2, 10, 50}, 100,000 steps): terminal
+                  v_y and yielded/unyielded field of FP32 against FP64, and
+                  the Bingham step's MLUPS
+  adjoint         lbm_adjoint on the adjoint workload (400x1200, one Bingham
+                  disk, 4000 steps, sqrt(N) checkpoints) against the forward
+                  time loop; gradients against FP64 central differences
+  batch           lbm_batch_step on 256 independent Bingham single-disk runs
+                  of uneven sizes against the same runs one after another
 
-Batch (N=1): the "batch" object times lbm_batch_step on 256 independent
-Bingham single-disk runs of uneven sizes (--batch-steps steps) against the
-same runs one after another through lbm_step.
+--profile-run CASE runs one workload for a few steps with no timing around
+it, for ncu captures of single launches: step-fp32 / step-fp64 (the bench
+workload), adjoint (the adjoint workload, objective over the last 100 steps),
+batch (the first --batch-sims runs of the batched workload, 32x8 tiles, 6
+blocks per SM).
 
 Multi-GPU: the hot path does not shard (one simulation, one GPU); --gpus N
 runs N independent replicas (weak scaling), timed as the max over ranks.
@@ -36,6 +46,7 @@ import argparse
 import importlib
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -48,29 +59,60 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_NODE = {0: 144.0, 1: 72.0}  # FP64 plain / FP32 shifted, Newtonian
+BINGHAM_BYTES_PER_NODE = {0: 160.0, 1: 80.0}  # + per-node omega read and written
 FALLBACK_HBM_GBS = 6650.0
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_step_fp32_sedimentation_1024x2048.md")
+# DRAM bytes (read + write) of one k_step<float> launch of the bench workload,
+# from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one launch, cold);
+# the capture and its command are in profiles/k_step_fp32_sedimentation_1024x2048.md
+K_STEP_FP32_TRAFFIC = {"bytes": 111724800.0, "captured_at": "11ba40b"}
+PARTS = ("fp32", "fp64", "e2e", "trajectory", "viscoplastic", "adjoint", "batch", "cpu")
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--parts", default="all",
+                    help="comma list of " + ",".join(PARTS) + " (default all; fp32 always runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint/forward time measurement")
-    ap.add_argument("--batch-steps", type=int, default=1000,
+    ap.add_argument("--batch-steps", type=int, default=20000,
                     help="steps of the 256-simulation batch measurement (0: skip)")
-    ap.add_argument("--accuracy-steps", type=int, default=2000,
+    ap.add_argument("--batch-seq-steps", type=int, default=1000,
+                    help="steps of each run alone (the sequential comparison)")
+    ap.add_argument("--batch-sims", type=int, default=256)
+    ap.add_argument("--accuracy-steps", type=int, default=50000,
                     help="steps of the FP32-vs-FP64 trajectory comparison (0: skip)")
+    ap.add_argument("--visco-steps", type=int, default=100000,
+                    help="steps of each viscoplastic-settling run (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="target CPU time of the bounded oracle sample")
     ap.add_argument("--nx", type=int, default=1024)
     ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--particles", type=int, default=512)
-    return ap.parse_args()
+    ap.add_argument("--profile-run", default="",
+                    choices=["", "step-fp32", "step-fp64", "adjoint", "batch"])
+    a = ap.parse_args(argv)
+    parts = set(PARTS) if a.parts == "all" else {s.strip() for s in a.parts.split(",") if s.strip()}
+    unknown = parts - set(PARTS)
+    if unknown:
+        ap.error(f"unknown parts: {sorted(unknown)}")
+    if a.no_cpu_baseline:
+        parts.discard("cpu")
+    if a.no_adjoint:
+        parts.discard("adjoint")
+    if a.batch_steps <= 0:
+        parts.discard("batch")
+    if a.accuracy_steps <= 0:
+        parts.discard("trajectory")
+    if a.visco_steps <= 0:
+        parts.discard("viscoplastic")
+    parts.add("fp32")
+    a.part_set = parts
+    return a
 
 
 def hbm_peak():
@@ -81,19 +123,6 @@ def hbm_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
-
-
-def profile_traffic():
-    """dram read+write bytes per launch of the FP32 lattice kernel from the
-    committed ncu summary (a line 'traffic_bytes_per_launch: N'), or None."""
-    try:
-        with open(PROFILE_TRAFFIC) as fh:
-            for line in fh:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
 
 
 class ClockSampler:
@@ -204,6 +233,13 @@ def job_mlups(world, nodes, steps, ms_max):
 
 
 def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False):
+    """Time args.steps steps of the bench workload with CUDA events on the
+    library's stream (state resident in HBM).  The step kernel and the
+    particle kernel of each step overlap (programmatic dependent launch), so
+    the step kernel's launches run back to back and their average duration
+    in the timed region is the timed region over the steps.  A second,
+    identical pass with events between the launches (which serialises them)
+    gives each kernel's own duration."""
     p, pin = workload(pkg, precision, args)
     p.device = device
     sim = pkg.Simulation(p)
@@ -219,9 +255,6 @@ def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False)
     clk = sampler.stop() if sampler else None
     ms = reduce_max(dist, torch, ms, f"cuda:{device}")
     status = sim.status()
-    # Per-kernel durations: an identical pass of the same number of steps
-    # with CUDA events recorded between the launches on the library's stream
-    # (events inside the timed pass itself would slow it by ~15%).
     sim.profile(True)
     sim.step(args.steps)
     (pms, lms), (pn, ln) = sim.profile_read()
@@ -231,7 +264,8 @@ def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False)
     sim.close()
     nodes = (p.nx + 1) * (p.ny + 1)
     return {
-        "ms": ms, "nodes": nodes, "lattice_ms": lms / max(ln, 1), "particle_ms": pms / max(pn, 1),
+        "ms": ms, "nodes": nodes, "lattice_ms_serialised": lms / max(ln, 1),
+        "particle_ms_serialised": pms / max(pn, 1),
         "launches": 2 * args.steps, "clocks": clk, "status": status,
         "finite": bool(np.all(np.isfinite(parts[:, :6]))),
     }
@@ -259,17 +293,18 @@ def run_e2e(pkg, torch, args, device):
     sim.step(args.warmup)
     sim.series()
     ext = torch.cuda.ExternalStream(sim.stream())
-    # (the host buffer the records land in is the caller's, allocated once)
+    # the host buffer the records land in is the caller's, allocated once
+    # before the time loop (pinned, so the drains copy straight into it)
+    rec_len = sim.series_record_len()
+    out = torch.empty((E2E_CHUNK, rec_len), dtype=torch.float64).pin_memory().numpy()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     k = args.steps
+    chunks = [min(E2E_CHUNK, k - s0) for s0 in range(0, k, E2E_CHUNK)]
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     t0.record(ext)
     sim.set_particles(pin_h)
-    chunks = [min(E2E_CHUNK, k - s0) for s0 in range(0, k, E2E_CHUNK)]
-    rec_len = sim.series_record_len()
-    out = torch.empty((E2E_CHUNK, rec_len), dtype=torch.float64).pin_memory().numpy()
     sim.step(chunks[0])
     for i, c in enumerate(chunks):
         if i + 1 < len(chunks):
@@ -296,28 +331,134 @@ def run_e2e(pkg, torch, args, device):
 
 def trajectory_error(pkg, args, device, steps):
     """FP32-shifted against FP64 plain on the bench workload, outside the
-    timed region: the largest disk displacement error after `steps` steps
+    timed region, at milestones up to `steps` steps (the multi-particle
+    configuration runs 50,000): the largest disk displacement error
     relative to the largest FP64 displacement, and the same for the velocity
     (the FP64 path matches the oracle within 1e-10 on the parity cases)."""
-    res = {}
+    sims = {}
     pin = None
     for prec in (1, 0):
         p, pin = workload(pkg, prec, args)
         p.device = device
-        sim = pkg.Simulation(p)
-        sim.set_particles(pin)
-        sim.step(steps)
-        res[prec] = sim.particles()
-        sim.close()
-    d32, d64 = res[1][:, 0:2] - pin[:, 0:2], res[0][:, 0:2] - pin[:, 0:2]
-    v32, v64 = res[1][:, 3:5], res[0][:, 3:5]
+        p.series_every = 0
+        sims[prec] = pkg.Simulation(p)
+        sims[prec].set_particles(pin)
+    marks = sorted({m for m in (2000, 10000, 20000, 30000, 40000, steps) if m <= steps})
     tiny = 1e-300
+    at = []
+    done = 0
+    for m in marks:
+        for s in sims.values():
+            s.step(m - done)
+        done = m
+        r32, r64 = sims[1].particles(), sims[0].particles()
+        d32, d64 = r32[:, 0:2] - pin[:, 0:2], r64[:, 0:2] - pin[:, 0:2]
+        v32, v64 = r32[:, 3:5], r64[:, 3:5]
+        at.append({
+            "steps": m,
+            "max_rel_displacement_err": float(np.max(np.linalg.norm(d32 - d64, axis=1)) /
+                                              max(float(np.max(np.linalg.norm(d64, axis=1))), tiny)),
+            "max_rel_velocity_err": float(np.max(np.linalg.norm(v32 - v64, axis=1)) /
+                                          max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)),
+            "max_fp64_displacement": float(np.max(np.linalg.norm(d64, axis=1))),
+            "status": [sims[1].status(), sims[0].status()],
+        })
+    for s in sims.values():
+        s.close()
+    last = at[-1]
     return {
         "steps": steps,
-        "max_rel_displacement_err": float(np.max(np.linalg.norm(d32 - d64, axis=1)) /
-                                          max(float(np.max(np.linalg.norm(d64, axis=1))), tiny)),
-        "max_rel_velocity_err": float(np.max(np.linalg.norm(v32 - v64, axis=1)) /
-                                      max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)),
+        "max_rel_displacement_err": last["max_rel_displacement_err"],
+        "max_rel_velocity_err": last["max_rel_velocity_err"],
+        "tolerance": 1e-4,
+        "within_tolerance": bool(last["max_rel_displacement_err"] <= 1e-4 and
+                                 last["max_rel_velocity_err"] <= 1e-4),
+        "milestones": at,
+    }
+
+
+VISCO_BN = (0.5, 2.0, 10.0, 50.0)
+
+
+def visco_measure(pkg, torch, device, steps, mlups_steps=4000):
+    """The viscoplastic-settling workload for each Bingham number: one FP32
+    and one FP64 run of `steps` steps (history every 10 steps, stress and
+    yield flags kept), compared by the disk's terminal v_y (mean over the
+    last tenth of the run) and by the yielded/unyielded flag of every fluid
+    node at the end (C6:947-954); then the Bingham step's MLUPS (80 B/node
+    FP32, 160 B/node FP64; no stress planes) over `mlups_steps` steps."""
+    cases = []
+    chunk = 10000
+    for bn in VISCO_BN:
+        res = {}
+        for prec in (1, 0):
+            p, pin, info = pkg.cases.workload_cfg3(prec, bn)
+            p.device = device
+            p.record_stress = 1
+            p.series_every = 10
+            p.series_particles = 1
+            p.series_capacity = chunk // 10 + 8
+            sim = pkg.Simulation(p)
+            sim.set_particles(pin)
+            hist = []
+            done = 0
+            while done < steps:
+                c = min(chunk, steps - done)
+                sim.step(c)
+                done += c
+                hist.append(sim.series())
+            h = np.concatenate(hist)
+            img = sim.image()
+            parts = sim.particles()
+            res[prec] = {"vy": h[:, 2 + 4], "y": h[:, 2 + 1], "img": img, "p": parts,
+                         "status": sim.status(), "u_ref": info["u_ref"], "tau_y": p.tau_y}
+            sim.close()
+        n = len(res[0]["vy"])
+        tail = slice(n - max(1, n // 10), n)
+        v32, v64 = float(np.mean(res[1]["vy"][tail])), float(np.mean(res[0]["vy"][tail]))
+        fluid = (res[0]["img"] != 10) & (res[1]["img"] != 10)
+        y32, y64 = res[1]["img"] == 5, res[0]["img"] == 5
+        agree = float(np.mean((y32 == y64)[fluid]))
+        traj = float(np.max(np.abs(res[1]["y"] - res[0]["y"])))
+        cases.append({
+            "bn": bn, "tau_y": res[0]["tau_y"], "u_ref": res[0]["u_ref"],
+            "terminal_vy_fp64": v64, "terminal_vy_fp32": v32,
+            "terminal_vy_over_u_ref_fp64": v64 / res[0]["u_ref"],
+            "terminal_vy_rel_err": abs(v32 - v64) / max(abs(v64), 1e-300),
+            "max_abs_y_err": traj,
+            "final_y_fp64": float(res[0]["p"][0, 1]), "final_y_fp32": float(res[1]["p"][0, 1]),
+            "unyielded_frac_fp64": float(np.mean(y64[fluid])),
+            "unyielded_frac_fp32": float(np.mean(y32[fluid])),
+            "yield_flag_agreement": agree,
+            "status": [res[1]["status"], res[0]["status"]],
+        })
+    # Bingham step throughput (no stress planes: the 80 / 160 B/node kernel)
+    rate = {}
+    for prec in (1, 0):
+        p, pin, _ = pkg.cases.workload_cfg3(prec, 2.0)
+        p.device = device
+        p.series_every = 10
+        p.series_capacity = 1024
+        sim = pkg.Simulation(p)
+        sim.set_particles(pin)
+        sim.step(20)
+        sim.series()
+        ms = time_steps(pkg, torch, sim, mlups_steps)
+        sim.series()
+        sim.close()
+        nodes = (p.nx + 1) * (p.ny + 1)
+        rate["fp32" if prec else "fp64"] = {
+            "mlups": nodes * mlups_steps / (ms * 1e-3) / 1e6,
+            "ms_per_step": ms / mlups_steps,
+            "bytes_per_node": BINGHAM_BYTES_PER_NODE[prec],
+            "achieved_gbs": BINGHAM_BYTES_PER_NODE[prec] * nodes / (ms / mlups_steps * 1e-3) / 1e9,
+        }
+    return {
+        "workload": "viscoplastic settling 800x2400 (1,923,201 nodes), one Bingham disk D=40 "
+                    "rho_p=2, tau_p=0.9, m=1e5, Bn = tau_y D/(nu U_ref), "
+                    "U_ref = D^2 (rho_p-1)|g|/nu, |g| from RE_S=0.78 as C6:27-29",
+        "steps": steps, "cases": cases, "step_rate": rate,
+        "terminal_window": "mean v_y over the last tenth of the run",
         "tolerance": 1e-4,
     }
 
@@ -374,8 +515,12 @@ def adjoint_measure(pkg, torch, device):
         return float(np.mean(v))
 
     fd = {}
-    for name in ("tau_y", "nu", "rho_p"):
-        base = {"tau_y": p64.tau_y, "nu": p64.nu, "rho_p": float(pin[0, 7])}[name]
+    names = ("tau_y", "nu", "rho_p", "x0", "y0")
+    col = {"rho_p": 7, "x0": 0, "y0": 1}
+    for name in names:
+        base = {"tau_y": p64.tau_y, "nu": p64.nu}.get(name, None)
+        if base is None:
+            base = float(pin[0, col[name]])
         d = 1e-4 * abs(base)
         jj = []
         for sgn in (1.0, -1.0):
@@ -386,12 +531,16 @@ def adjoint_measure(pkg, torch, device):
             elif name == "nu":
                 q.nu = base + sgn * d
             else:
-                disks[0, 7] = base + sgn * d
+                disks[0, col[name]] = base + sgn * d
             jj.append(run_j(q, disks))
         fd[name] = (jj[0] - jj[1]) / (2 * d)
     j32, g32 = res[1]
     j64, g64 = res[0]
-    pick = lambda g, k: float(g[k] if k != "rho_p" else g[k][0])  # noqa: E731
+    pick = lambda g, k: float(g[k] if k in ("tau_y", "nu") else g[k][0])  # noqa: E731
+    # dJ/dx0 vanishes by symmetry (the disk starts on the vertical centre
+    # line): it is judged against the scale of dJ/dy0, the others relatively
+    rel = [k for k in fd if k != "x0"]
+    scale_x = abs(fd["y0"])
     out.update({
         "workload": "Bingham settling 400x1200 (481,601 nodes), disk D=24 rho_p=1.5, Bn=5, "
                     "tau_p=0.9, m=1e5, 4000 steps, J = mean v_y over steps 3000..4000",
@@ -400,21 +549,28 @@ def adjoint_measure(pkg, torch, device):
         "grad_fp32": {k: pick(g32, k) for k in fd},
         "grad_fp64": {k: pick(g64, k) for k in fd},
         "fd_fp64": fd,
-        "max_rel_err_fp32_vs_fd": max(abs(pick(g32, k) - fd[k]) / abs(fd[k]) for k in fd),
-        "max_rel_err_fp64_vs_fd": max(abs(pick(g64, k) - fd[k]) / abs(fd[k]) for k in fd),
+        "fd_rel_step": 1e-4,
+        "max_rel_err_fp32_vs_fd": max(abs(pick(g32, k) - fd[k]) / abs(fd[k]) for k in rel),
+        "max_rel_err_fp64_vs_fd": max(abs(pick(g64, k) - fd[k]) / abs(fd[k]) for k in rel),
         "max_rel_err_fp32_vs_fp64_adjoint": max(abs(pick(g32, k) - pick(g64, k)) /
-                                                abs(pick(g64, k)) for k in fd),
+                                                abs(pick(g64, k)) for k in rel),
+        "x0_abs_err_over_dJdy0": {
+            "fp32_vs_fd": abs(pick(g32, "x0") - fd["x0"]) / scale_x,
+            "fp64_vs_fd": abs(pick(g64, "x0") - fd["x0"]) / scale_x,
+        },
         "tolerance": 1e-3,
     })
     return out
 
 
-def batch_measure(pkg, torch, device, steps):
+def batch_measure(pkg, torch, device, steps, seq_steps, nsim=256):
     """The batched workload (256 seeded Bingham single-disk runs, widths
     128..512, heights 3x, FP32): one lbm_batch_step of `steps` steps (after
-    the tuning steps) against each run alone through lbm_step for the same
-    steps; CUDA events on the batch's / each handle's stream."""
-    cs = pkg.cases.workload_cfg4(1)
+    the tuning steps) against each run alone through lbm_step for
+    `seq_steps` steps (the per-step rate of a run alone is steady after its
+    warm-up, so its time for `steps` steps is scaled from those); CUDA events
+    on the batch's / each handle's stream."""
+    cs = pkg.cases.workload_cfg4(1)[:nsim]
     for p, _ in cs:
         p.device = device
     nodes = [(p.nx + 1) * (p.ny + 1) for p, _ in cs]
@@ -433,6 +589,7 @@ def batch_measure(pkg, torch, device, steps):
     batch_ms = e0.elapsed_time(e1)
     tuning = b.tuning()
     finite = all(np.all(np.isfinite(s.particles())) for s in b.sims)
+    status = max(abs(s.status()) for s in b.sims)
     b.close()
     alone = []
     for p, pin in cs:
@@ -442,26 +599,41 @@ def batch_measure(pkg, torch, device, steps):
         ext = torch.cuda.ExternalStream(sim.stream())
         torch.cuda.synchronize()
         e0.record(ext)
-        sim.step(steps)
+        sim.step(seq_steps)
         e1.record(ext)
         e1.synchronize()
-        alone.append(e0.elapsed_time(e1))
+        alone.append(e0.elapsed_time(e1) * steps / seq_steps)
         sim.close()
     alone = np.array(alone)
     total = float(np.sum(nodes)) * steps
     return {
-        "workload": "256 Bingham single-disk runs (C6), W ~ U[128,512], H = 3W, D = W/10, "
+        "workload": f"{len(cs)} Bingham single-disk runs (C6), W ~ U[128,512], H = 3W, D = W/10, "
                     "Bn log-uniform [0.1,100], rho_p ~ U[1.2,3], tau_p 0.9, m 1e5, seed 0, FP32",
         "simulations": len(cs), "nodes": int(np.sum(nodes)), "steps": steps,
         "tile": list(tuning[:2]), "blocks_per_sm": tuning[2],
         "batch_ms": batch_ms, "batch_mlups": total / (batch_ms * 1e-3) / 1e6,
+        "roofline_frac_80B": total / (batch_ms * 1e-3) * 80.0 / 1e9 / hbm_peak()[0],
         "per_sim_wall_ms_batched": batch_ms,
         "sequential_ms": float(np.sum(alone)),
         "sequential_mlups": total / (float(np.sum(alone)) * 1e-3) / 1e6,
+        "sequential_measured_steps": seq_steps,
         "alone_ms_p50": float(np.percentile(alone, 50)), "alone_ms_p99": float(np.percentile(alone, 99)),
         "speedup_vs_sequential": float(np.sum(alone)) / batch_ms,
-        "finite": bool(finite),
+        "finite": bool(finite), "status": -status,
     }
+
+
+def host_cpu():
+    model = platform.processor() or "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return model, os.cpu_count() or 0
 
 
 def cpu_baseline(pkg, args, seconds):
@@ -491,10 +663,13 @@ def cpu_baseline(pkg, args, seconds):
     o.step(n)
     dt = time.perf_counter() - t
     o.close()
+    model, ncpu = host_cpu()
     return {
         "value": nodes * n / dt / 1e6,
         "unit": "MLUPS",
         "cores": 1,
+        "host_cpu": model,
+        "host_nproc": ncpu,
         "kind": "port",
         "sample": (f"{n} full time steps of the {args.nx}x{args.ny}, {len(pin)}-disk workload "
                    f"after 1 untimed step ({dt:.1f} s); PHI "
@@ -535,6 +710,9 @@ def main():
 
     import torch
 
+    if args.profile_run:
+        return profile_run(pkg, args)
+
     dist = None
     if world > 1:
         import torch.distributed as tdist
@@ -544,18 +722,21 @@ def main():
         tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
         dist = tdist
     device = local if world > 1 else 0
+    parts = args.part_set
 
     r32 = run_gpu_path(pkg, torch, args, 1, device, world, dist, clocks=True)
-    r64 = run_gpu_path(pkg, torch, args, 0, device, world, dist)
-    e2e = run_e2e(pkg, torch, args, device)
-    if dist is not None:
+    r64 = run_gpu_path(pkg, torch, args, 0, device, world, dist) if "fp64" in parts else None
+    e2e = run_e2e(pkg, torch, args, device) if "e2e" in parts else None
+    if dist is not None and e2e is not None:
         e2e["value"] = world / reduce_max(dist, torch, 1.0 / e2e["value"], f"cuda:{device}")
 
     peak, peak_src = hbm_peak()
-    ach32 = BYTES_PER_NODE[1] * r32["nodes"] / (r32["lattice_ms"] * 1e-3) / 1e9
-    ach64 = BYTES_PER_NODE[0] * r64["nodes"] / (r64["lattice_ms"] * 1e-3) / 1e9
+    # the step kernel's average launch duration in the timed region: its
+    # launches run back to back (the particle kernel overlaps them), so it is
+    # the timed region over the steps
+    kms32 = r32["ms"] / args.steps
+    ach32 = BYTES_PER_NODE[1] * r32["nodes"] / (kms32 * 1e-3) / 1e9
     value = job_mlups(world, r32["nodes"], args.steps, r32["ms"])
-    value64 = job_mlups(world, r64["nodes"], args.steps, r64["ms"])
     line = {
         "metric": metric,
         "value": value,
@@ -563,7 +744,7 @@ def main():
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": r32["ms"] / args.steps,
+        "ms_per_step": kms32,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -576,39 +757,91 @@ def main():
             "peak": peak,
             "unit": "GB/s",
             "frac": ach32 / peak,
-            "traffic": profile_traffic(),
+            "traffic": K_STEP_FP32_TRAFFIC["bytes"],
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                               "k_step<float> launch of this workload, captured at commit "
+                               + K_STEP_FP32_TRAFFIC["captured_at"]),
             "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
             else "fallback 6.65 TB/s",
             "bytes_per_node": BYTES_PER_NODE[1],
             "kernel": "k_step<float>",
-            "kernel_ms": r32["lattice_ms"],
-            "particle_kernel_ms": r32["particle_ms"],
+            "kernel_ms": kms32,
+            "kernel_ms_source": "timed region / steps (launches back to back, CUDA events "
+                                "on the library stream)",
+            "kernel_ms_serialised": r32["lattice_ms_serialised"],
+            "particle_kernel_ms_serialised": r32["particle_ms_serialised"],
+            "serialised_source": "an identical pass with CUDA events between the launches, "
+                                 "which serialises the step and particle kernels",
         },
-        "fp64": {
-            "value": value64, "unit": "MLUPS", "ms_per_step": r64["ms"] / args.steps,
-            "roofline_frac": ach64 / peak, "achieved_gbs": ach64,
-            "kernel_ms": r64["lattice_ms"], "bytes_per_node": BYTES_PER_NODE[0],
-        },
-        "fp32_over_fp64": value / value64,
-        "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
         "gpu_launches": r32["launches"],
         "clocks": r32["clocks"],
-        "status": {"fp32": r32["status"], "fp64": r64["status"],
-                   "finite": r32["finite"] and r64["finite"]},
+        "status": {"fp32": r32["status"], "finite": r32["finite"]},
     }
-    if args.accuracy_steps > 0:
+    if r64 is not None:
+        kms64 = r64["ms"] / args.steps
+        ach64 = BYTES_PER_NODE[0] * r64["nodes"] / (kms64 * 1e-3) / 1e9
+        value64 = job_mlups(world, r64["nodes"], args.steps, r64["ms"])
+        line["fp64"] = {
+            "value": value64, "unit": "MLUPS", "ms_per_step": kms64,
+            "roofline_frac": ach64 / peak, "achieved_gbs": ach64,
+            "kernel_ms_serialised": r64["lattice_ms_serialised"],
+            "bytes_per_node": BYTES_PER_NODE[0],
+        }
+        line["fp32_over_fp64"] = value / value64
+        line["status"]["fp64"] = r64["status"]
+        line["status"]["finite"] = r32["finite"] and r64["finite"]
+    if e2e is not None:
+        line["e2e"] = {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step",
+                                           "d2h_bytes_per_step")}
+        line["e2e"]["output"] = e2e["output"]
+    if world == 1 and "trajectory" in parts:
         line["trajectory_err"] = trajectory_error(pkg, args, device, args.accuracy_steps)
-    if world == 1 and not args.no_adjoint:
+    if world == 1 and "viscoplastic" in parts:
+        line["viscoplastic"] = visco_measure(pkg, torch, device, args.visco_steps)
+    if world == 1 and "adjoint" in parts:
         line["adjoint"] = adjoint_measure(pkg, torch, device)
-    if world == 1 and args.batch_steps > 0:
-        line["batch"] = batch_measure(pkg, torch, device, args.batch_steps)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if world == 1 and "batch" in parts:
+        line["batch"] = batch_measure(pkg, torch, device, args.batch_steps, args.batch_seq_steps,
+                                      args.batch_sims)
+    if rank == 0 and world == 1 and "cpu" in parts:
         line["cpu_baseline"] = cpu_baseline(pkg, args, args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def profile_run(pkg, args):
+    """A short run of one workload with no timing around it (ncu captures)."""
+    if args.profile_run == "adjoint":
+        p, pin, _ = pkg.cases.workload_cfg5(1)
+        with pkg.Simulation(p) as sim:
+            sim.set_particles(pin)
+            j, g = sim.adjoint(max(1, args.steps - 100), args.steps)
+            print(f"steps {sim.kk}  J {j:.9e}  dJ/dtau_y {g['tau_y']:.9e}  status {sim.status()}")
+        return 0
+    if args.profile_run == "batch":
+        cs = pkg.cases.workload_cfg4(1)[: args.batch_sims]
+        b = pkg.Batch([q for q, _ in cs])
+        b.set_tuning(32, 8, 6)
+        for s, (_, disks) in zip(b.sims, cs):
+            s.set_particles(disks)
+        b.step(args.steps)
+        parts = b.sims[0].particles()
+        print(f"steps {b.sims[0].kk}  run 0 disk at ({parts[0, 0]:.6f}, {parts[0, 1]:.6f})  "
+              f"status {max(abs(s.status()) for s in b.sims)}")
+        b.close()
+        return 0
+    prec = 1 if args.profile_run == "step-fp32" else 0
+    p, pin = workload(pkg, prec, args)
+    with pkg.Simulation(p) as sim:
+        sim.set_particles(pin)
+        sim.step(args.steps)
+        parts = sim.particles()
+        print(f"steps {sim.kk}  disk 0 at ({parts[0, 0]:.6f}, {parts[0, 1]:.6f})  "
+              f"status {sim.status()}")
+    return 0
 
 
 if __name__ == "__main__":

@@ -39,9 +39,13 @@ enum {
     LBM_E_CUDA = -4,      /* CUDA runtime error (no device, launch failure)   */
     LBM_E_NAN = -5,       /* non-finite density or particle state detected    */
     LBM_E_TIMEOUT = -6,   /* a bounded device-side wait gave up               */
-    LBM_E_OVERFLOW = -7,  /* a lattice tile is touched by too many particles  */
+    LBM_E_OVERFLOW = -7,  /* a fixed capacity exceeded: too many particles on
+                             one lattice tile or near one particle, or (FP32)
+                             a node's |rho - rho0| >= 2, beyond the range of
+                             the mean-density sum                             */
     LBM_E_STATE = -8,     /* call out of order (e.g. step before particles)   */
-    LBM_E_PARTICLE = -9,  /* particle outside the lattice                     */
+    LBM_E_PARTICLE = -9,  /* particle outside the lattice, or input disks that
+                             overlap (lbm_set_particles)                      */
     LBM_E_ABI = -10,      /* struct_size does not match this library          */
     LBM_E_SCRATCH = -11   /* input larger than lbm_fields_noalloc's scratch   */
 };
@@ -359,10 +363,14 @@ int lbm_batch_destroy(lbm_batch* b);
  * LBM_E_SCRATCH before any work is queued.  Each call clears the scratch it
  * uses, so nothing needs to start at zero.  The first call on a device also
  * looks up the scratch address (make it before any stream capture starts on
- * that device).  The scratch is shared by all calls on a device: calls that
- * overlap in time on one device race and must be serialised by the caller.
- * The call returns after its work on `stream` has finished; LBM_E_OVERFLOW
- * if more than 32 disks touch one tile. */
+ * that device); after cudaDeviceReset the next call looks it up again.  The
+ * scratch is shared by all calls on a device: calls that overlap in time on
+ * one device race and must be serialised by the caller.  The call returns
+ * after its work on `stream` has finished.  LBM_E_OVERFLOW: more than 32
+ * disks touch one tile; out is then incomplete (the disks past the 32nd of
+ * that tile are left out of its PHI, G and image).  LBM_E_NAN: a particle
+ * record holds a non-finite position, velocity or diameter; that disk is
+ * left out of out. */
 #define LBM_NOALLOC_MAX_TILES 16384
 #define LBM_NOALLOC_MAX_PARTICLES 4096
 int lbm_fields_noalloc(const lbm_params* p, const double* f, int32_t np,

@@ -130,9 +130,12 @@ def run_case(ref_root, name, spec):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("LBM_REFERENCE_DIR"),
+                    help="root of the reference project (or LBM_REFERENCE_DIR)")
     ap.add_argument("--case", action="append")
     a = ap.parse_args(argv)
+    if not a.reference:
+        ap.error("give --reference or set LBM_REFERENCE_DIR")
     for name, spec in CASES.items():
         if a.case and name not in a.case:
             continue

@@ -86,3 +86,43 @@ def test_noalloc_rejects_oversize_before_any_work(pkg):
     rc = lib.lbm_fields_noalloc(ctypes.byref(p), dummy, 4097, dummy, dummy, None)
     assert rc == -11
     assert lib.lbm_fields_noalloc(ctypes.byref(p), None, 0, None, dummy, None) == -1
+
+
+def _raw_call(pkg, torch, params, f, pin):
+    n1x, n1y = params.nx + 1, params.ny + 1
+    dev = torch.device("cuda", 0)
+    f_d = torch.from_numpy(np.ascontiguousarray(f)).to(dev)
+    pin_d = torch.from_numpy(np.ascontiguousarray(pin).reshape(-1)).to(dev)
+    out_d = torch.zeros((7 * n1x * n1y,), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    lib = pkg.load_library()
+    rc = lib.lbm_fields_noalloc(
+        ctypes.byref(params), ctypes.c_void_p(f_d.data_ptr()), pin.shape[0],
+        ctypes.c_void_p(pin_d.data_ptr()), ctypes.c_void_p(out_d.data_ptr()),
+        ctypes.c_void_p(stream.cuda_stream))
+    return rc, out_d.cpu().numpy().reshape(7, n1y, n1x)
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_overflow_and_nonfinite_records(pkg, cases):
+    """33 small disks in one 128 x 8 tile: LBM_E_OVERFLOW (the output is
+    then incomplete).  A record with a non-finite position: LBM_E_NAN, the
+    other disks still evaluated.  A clean call afterwards returns 0: the
+    flags of the scratch start at zero on every call."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    p = cases.shipped_c1(200, 40, 2.0)
+    n = (p.nx + 1) * (p.ny + 1)
+    f = np.tile(np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4), n)  # rest state
+    many = cases.pin_array([[3.0 + 3.0 * k, 4.0] for k in range(33)], 2.0, 1.25)
+    rc, _ = _raw_call(pkg, torch, p, f, many)
+    assert rc == -7
+    bad = cases.pin_array([[30.0, 20.0], [60.0, 20.0]], 8.0, 1.25)
+    bad[1, 0] = np.nan
+    rc, out = _raw_call(pkg, torch, p, f, bad)
+    assert rc == -5
+    assert out[3, 20, 30] == 1.0  # the finite disk's centre is solid
+    rc, out = _raw_call(pkg, torch, p, f, bad[:1])
+    assert rc == 0
+    assert out[3, 20, 30] == 1.0 and out[3, 20, 60] == 0.0
