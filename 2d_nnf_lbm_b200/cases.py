@@ -214,9 +214,11 @@ def shipped_c3(nx: int = 512, ny: int = 512) -> LbmParams:
 
 
 # ---- benchmark workloads ------------------------------------------------------
-# cfg1: gravity tuned once on the FP64 oracle/GPU so that the terminal
-# Re_p = rho_p*D*|v|/NU (C1:261) is about 20; frozen here as a constant.
-CFG1_GRAVITY = -6.0e-4
+# cfg1: gravity tuned once on the FP64 oracle (tests/golden/make_cfg1.py --tune)
+# so that the particle Reynolds number Re_p = rho_p*D*|v|/NU of C1:261
+# peaks at about 20 during the fall (19.96, at step ~7170, just before the
+# bottom wall slows the disk); frozen here as a constant.
+CFG1_GRAVITY = -5.125e-4
 
 
 def workload_cfg1(precision: int = LBM_FP64) -> tuple[LbmParams, np.ndarray]:

@@ -131,3 +131,43 @@ def test_batch_rejects_mixed_precision(pkg, cases):
     with pytest.raises(pkg.LbmError):
         b = pkg.Batch([p])
         b.set_tuning(48, 4, 2)
+
+
+@pytest.mark.parametrize("precision,rtol", [(0, 1e-10), (1, 1e-4)])
+def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol):
+    """Each MRT run of a batch (the batched kernel's one-node-per-thread tile
+    body) against the oracle's run of the same inputs, not against another
+    GPU path: the C6 Bingham case (the GPU's per-node omega, oracle rule
+    omega_chain=0, 1e-8 in FP64 as in the single-run parity tests), C1
+    Zou-He and a C3 pair in contact range."""
+    from oracle.oracle import Oracle
+
+    cs = []
+    for name in ("c6_bingham", "c1_newton", "c3_pair"):
+        p, pin, _, _ = ac.build(cases, name)
+        p = p.copy(precision=precision)
+        p.series_every = 0
+        cs.append((name, p, pin))
+    steps = 41
+    b = pkg.Batch([p for _, p, _ in cs])
+    for s, (_, _, pin) in zip(b.sims, cs):
+        s.set_particles(pin)
+    b.step(steps)
+    for s, (name, p, pin) in zip(b.sims, cs):
+        tol = 1e-8 if (precision == 0 and name == "c6_bingham") else rtol
+        ref = Oracle(p, omega_chain=0)
+        ref.set_particles(pin)
+        ref.step(steps)
+        gp, rp = s.particles(), ref.particles()
+        d = float(np.max(pin[:, 6]))
+        vmax = max(float(np.max(np.abs(rp[:, 3:5]))), 1e-300)
+        disp = max(float(np.max(np.abs(rp[:, 0:2] - pin[:, 0:2]))), 1e-300)
+        assert np.max(np.abs(gp[:, 0:2] - rp[:, 0:2])) <= tol * disp, (name, "position")
+        assert np.max(np.abs(gp[:, 3:5] - rp[:, 3:5])) <= tol * vmax, (name, "velocity")
+        assert np.max(np.abs(gp[:, 5] - rp[:, 5])) <= tol * vmax / d, (name, "spin")
+        for fld in ("ux", "uy", "rho"):  # each against its field's magnitude
+            g, r = s.field(fld), ref.field(fld)
+            sc = float(np.max(np.abs(r)))
+            assert np.max(np.abs(g - r)) <= tol * max(sc, 1e-300), (name, fld)
+        ref.close()
+    b.close()
