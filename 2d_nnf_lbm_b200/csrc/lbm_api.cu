@@ -1797,14 +1797,19 @@ extern "C" int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, 
 // ===========================================================================
 // Batched time steps.  All simulations of a batch advance in lockstep on the
 // batch's stream: per step one launch of k_particles_batch (block b =
-// simulation b) and one of k_lattice_batch (persistent grid over every
-// simulation's tiles).  Steps run from a captured graph of BATCH_GRAPH_STEPS
-// steps once the tile shape and grid are chosen.
+// simulation b) and one of the batched lattice kernel: k_step_batch (the
+// TMA-staged tiles of the step kernel) or k_lattice_batch (one node per
+// thread, any tile shape; the only one for BGK runs), whichever the
+// autotuner timed fastest.  Steps run from a captured graph of
+// BATCH_GRAPH_STEPS steps once the kernel, tile shape and grid are chosen.
 struct lbm_batch {
   std::vector<lbm_sim*> sims;
   int device = 0;
   int prec = 0;
   int bgk = 0;             // some simulation uses the BGK collision
+  int stress = 0;          // some simulation needs the strain rate (TMA kernel variant)
+  int tma_bpsm = 0;        // resident blocks per SM of the TMA-staged kernel (0: not usable)
+  CUtensorMap* d_tmaps = nullptr;  // [2 nsim]: each simulation's f[0], f[1]
   int nsm = 148;
   cudaStream_t stream = nullptr;
   BatchSim* d_sims = nullptr;
@@ -1826,14 +1831,23 @@ constexpr int BATCH_GRAPH_STEPS = 8;
 constexpr int BATCH_BPSM[3] = {2, 4, 6};
 
 int batch_grid(const lbm_batch* b) {
-  const long long g = (long long)b->bpsm * b->nsm;
+  const long long g = (long long)(b->shape == BATCH_SHAPE_TMA ? b->tma_bpsm : b->bpsm) * b->nsm;
   return (int)std::max<long long>(1, std::min<long long>(g, b->total));
 }
 
 // Per-simulation arguments at tile shape `shape`, uploaded to the device.
+// Tile width and height of shape (the TMA shape's depend on the precision).
+int batch_tile_x(const lbm_batch* b, int shape) {
+  return shape == BATCH_SHAPE_TMA ? step_tile_width(b->prec == LBM_FP64 ? 8 : 4)
+                                  : batch_bx(shape);
+}
+int batch_tile_y(const lbm_batch* b, int shape) {
+  return shape == BATCH_SHAPE_TMA ? step_box_rows(b->prec == LBM_FP64 ? 8 : 4) : batch_by(shape);
+}
+
 int batch_upload(lbm_batch* b, int shape) {
   const int n = (int)b->sims.size();
-  const int bx = batch_bx(shape), by = batch_by(shape);
+  const int bx = batch_tile_x(b, shape), by = batch_tile_y(b, shape);
   long long first = 0;
   for (int q = 0; q < n; ++q) {
     lbm_sim* h = b->sims[q];
@@ -1861,14 +1875,23 @@ int batch_upload(lbm_batch* b, int shape) {
   return LBM_OK;
 }
 
+cudaError_t batch_launch_lattice(lbm_batch* b) {
+  const int n = (int)b->sims.size();
+  if (b->shape == BATCH_SHAPE_TMA)
+    return b->prec == LBM_FP64 ? launch_batch_tma_fp64(b->d_sims, n, b->d_tmaps, b->total,
+                                                       b->stress, batch_grid(b), b->stream)
+                               : launch_batch_tma_fp32(b->d_sims, n, b->d_tmaps, b->total,
+                                                       b->stress, batch_grid(b), b->stream);
+  return b->prec == LBM_FP64 ? launch_batch_fp64(b->d_sims, n, b->total, b->shape, b->bgk,
+                                                 batch_grid(b), b->stream)
+                             : launch_batch_fp32(b->d_sims, n, b->total, b->shape, b->bgk,
+                                                 batch_grid(b), b->stream);
+}
+
 cudaError_t batch_launch_step(lbm_batch* b) {
   cudaError_t e = launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream);
   if (e != cudaSuccess) return e;
-  return b->prec == LBM_FP64
-             ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, b->shape, b->bgk,
-                                 batch_grid(b), b->stream)
-             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, b->shape, b->bgk,
-                                 batch_grid(b), b->stream);
+  return batch_launch_lattice(b);
 }
 
 // Host bookkeeping of s completed batch steps.
@@ -1895,21 +1918,25 @@ long long batch_room(const lbm_batch* b) {
 }
 
 int batch_tune(lbm_batch* b, int32_t& left) {
-  // one timed step per (shape, blocks per SM), results independent of both
+  // one timed step per candidate: the TMA-staged kernel (MRT batches), then
+  // each (shape, blocks per SM) of the one-node-per-thread kernel; results
+  // do not depend on the choice
   float best = 1e30f;
   int bs = 0, bb = BATCH_BPSM[0];
-  for (int sh = 0; sh < BATCH_SHAPES && left > 0; ++sh) {
+  std::vector<int> shapes;
+  if (b->tma_bpsm > 0) shapes.push_back(BATCH_SHAPE_TMA);
+  for (int sh = 0; sh < BATCH_SHAPES; ++sh) shapes.push_back(sh);
+  for (const int sh : shapes) {
+    if (left <= 0) break;
     int rc = batch_upload(b, sh);
     if (rc) return rc;
     b->shape = sh;
-    for (int k = 0; k < 3 && left > 0 && batch_room(b) > 0; ++k) {
-      b->bpsm = BATCH_BPSM[k];
+    const int ngrid = sh == BATCH_SHAPE_TMA ? 1 : 3;
+    for (int k = 0; k < ngrid && left > 0 && batch_room(b) > 0; ++k) {
+      b->bpsm = sh == BATCH_SHAPE_TMA ? b->tma_bpsm : BATCH_BPSM[k];
       CK(launch_particles_batch(b->d_pargs, (int)b->sims.size(), b->stream));
       CK(cudaEventRecord(b->ev[0], b->stream));
-      CK(b->prec == LBM_FP64 ? launch_batch_fp64(b->d_sims, (int)b->sims.size(), b->total, sh,
-                                                 b->bgk, batch_grid(b), b->stream)
-                             : launch_batch_fp32(b->d_sims, (int)b->sims.size(), b->total, sh,
-                                                 b->bgk, batch_grid(b), b->stream));
+      CK(batch_launch_lattice(b));
       CK(cudaEventRecord(b->ev[1], b->stream));
       CK(cudaEventSynchronize(b->ev[1]));
       float ms = 0.f;
@@ -1919,7 +1946,7 @@ int batch_tune(lbm_batch* b, int32_t& left) {
       if (ms < best) {
         best = ms;
         bs = sh;
-        bb = BATCH_BPSM[k];
+        bb = b->bpsm;
       }
       // the next launch decodes the force sums this one left
       for (ParticleArgs& pa : b->h_pargs) pa.decode_force = 1;
@@ -1969,6 +1996,23 @@ int lbm_batch_create(const lbm_params* params, int32_t nsim, lbm_batch** out) {
   if ((rc = dalloc(&b->d_sims, nsim)) || (rc = dalloc(&b->d_pargs, nsim))) return fail(rc);
   b->h_sims.resize(nsim);
   b->h_pargs.resize(nsim);
+  // the TMA-staged kernel: every simulation's tensor maps, and its occupancy
+  // (which also sets its shared-memory size, before any graph capture)
+  for (lbm_sim* h : b->sims) b->stress |= (h->m.bingham || h->m.record_stress) ? 1 : 0;
+  if (!b->bgk) {
+    std::vector<CUtensorMap> tm(2 * (size_t)nsim);
+    for (int q = 0; q < nsim; ++q) {
+      tm[2 * (size_t)q] = b->sims[q]->tm[0];
+      tm[2 * (size_t)q + 1] = b->sims[q]->tm[1];
+    }
+    if ((rc = dalloc(&b->d_tmaps, tm.size()))) return fail(rc);
+    if (cudaMemcpy(b->d_tmaps, tm.data(), tm.size() * sizeof(CUtensorMap),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(LBM_E_CUDA);
+    const cudaError_t e = b->prec == LBM_FP64 ? batch_tma_prepare_fp64(b->stress, &b->tma_bpsm)
+                                              : batch_tma_prepare_fp32(b->stress, &b->tma_bpsm);
+    if (e != cudaSuccess) return fail(cuda_fail(e));
+  }
   *out = b;
   return LBM_OK;
 }
@@ -1980,8 +2024,8 @@ lbm_sim* lbm_batch_sim(lbm_batch* b, int32_t i) {
 
 int lbm_batch_tuning(lbm_batch* b, int32_t* tile_x, int32_t* tile_y, int32_t* blocks_per_sm) {
   if (!b || !tile_x || !tile_y || !blocks_per_sm) return LBM_E_INVALID;
-  *tile_x = b->shape < 0 ? 0 : batch_bx(b->shape);
-  *tile_y = b->shape < 0 ? 0 : batch_by(b->shape);
+  *tile_x = b->shape < 0 ? 0 : batch_tile_x(b, b->shape);
+  *tile_y = b->shape < 0 ? 0 : batch_tile_y(b, b->shape);
   *blocks_per_sm = b->shape < 0 ? 0 : b->bpsm;
   return LBM_OK;
 }
@@ -1996,6 +2040,14 @@ int lbm_batch_set_tuning(lbm_batch* b, int32_t tile_x, int32_t tile_y, int32_t b
   int sh = -1;
   for (int q = 0; q < BATCH_SHAPES; ++q)
     if (batch_bx(q) == tile_x && batch_by(q) == tile_y) sh = q;
+  // the TMA-staged tiles run at their own occupancy (blocks_per_sm ignored)
+  if (b->tma_bpsm > 0 && tile_x == batch_tile_x(b, BATCH_SHAPE_TMA) &&
+      tile_y == batch_tile_y(b, BATCH_SHAPE_TMA)) {
+    b->shape = BATCH_SHAPE_TMA;
+    b->bpsm = b->tma_bpsm;
+    b->fixed = true;
+    return LBM_OK;
+  }
   if (sh < 0 || blocks_per_sm < 1 || blocks_per_sm > 64) return LBM_E_INVALID;
   b->shape = sh;
   b->bpsm = blocks_per_sm;
@@ -2092,6 +2144,7 @@ int lbm_batch_destroy(lbm_batch* b) {
   for (lbm_sim* h : b->sims) lbm_destroy(h);
   dfree(b->d_sims);
   dfree(b->d_pargs);
+  dfree(b->d_tmaps);
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);

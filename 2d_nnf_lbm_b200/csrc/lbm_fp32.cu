@@ -36,6 +36,13 @@ cudaError_t launch_wait_selftest(int* status, uint32_t limit, cudaStream_t s) {
   k_wait_selftest<<<1, 32, 0, s>>>(status, limit);
   return cudaGetLastError();
 }
+cudaError_t launch_batch_tma_fp32(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
+                                  long long total, int stress, int grid, cudaStream_t s) {
+  return launch_batch_tma<float>(sims, nsim, tmaps, total, stress, grid, s);
+}
+cudaError_t batch_tma_prepare_fp32(int stress, int* blocks_per_sm) {
+  return batch_tma_prepare<float>(stress, blocks_per_sm);
+}
 cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_STEP);
 }

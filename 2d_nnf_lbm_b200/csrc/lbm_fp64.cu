@@ -21,6 +21,13 @@ cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, i
                               int bgk, int grid, cudaStream_t s) {
   return launch_batch<double>(sims, nsim, total, shape, bgk, grid, s);
 }
+cudaError_t launch_batch_tma_fp64(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
+                                  long long total, int stress, int grid, cudaStream_t s) {
+  return launch_batch_tma<double>(sims, nsim, tmaps, total, stress, grid, s);
+}
+cudaError_t batch_tma_prepare_fp64(int stress, int* blocks_per_sm) {
+  return batch_tma_prepare<double>(stress, blocks_per_sm);
+}
 cudaError_t launch_bgk_step_fp64(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<double>(a, s, MODE_STEP);
 }

@@ -207,7 +207,8 @@ cudaError_t launch_bgk_step_fp32(const LatticeArgs& a, cudaStream_t s);
 
 // TMA box of the step kernel: one tile row (128 FP32 / 64 FP64 nodes) plus
 // a 16-byte vector of halo on each side; 512 / row-width rows; one plane.
-inline int step_box_width(int esz) { return (esz == 8 ? 64 : 128) + 2 * (16 / esz); }
+inline int step_tile_width(int esz) { return esz == 8 ? 64 : 128; }
+inline int step_box_width(int esz) { return step_tile_width(esz) + 2 * (16 / esz); }
 inline int step_box_rows(int esz) { return 512 / (esz == 8 ? 64 : 128); }
 
 // Particle kernel (lbm_particles.cu).
@@ -235,8 +236,11 @@ struct BatchSim {
   long long first;     // first work item of this simulation
 };
 
-// Batch tile shapes (nodes): 0: 32 x 8, 1: 64 x 4, 2: 128 x 2.
+// Batch tile shapes (nodes): 0: 32 x 8, 1: 64 x 4, 2: 128 x 2 (one node per
+// thread); BATCH_SHAPE_TMA: the TMA-staged tiles of the step kernel (128 x 4
+// FP32, 64 x 8 FP64), MRT models only.
 constexpr int BATCH_SHAPES = 3;
+constexpr int BATCH_SHAPE_TMA = 3;
 __host__ __device__ constexpr int batch_bx(int shape) { return shape == 0 ? 32 : (shape == 1 ? 64 : 128); }
 __host__ __device__ constexpr int batch_by(int shape) { return 256 / batch_bx(shape); }
 
@@ -244,6 +248,16 @@ cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, i
                               int bgk, int grid, cudaStream_t s);
 cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
                               int bgk, int grid, cudaStream_t s);
+// The TMA-staged batched step: tensor maps of f[0], f[1] per simulation
+// (tmaps[2 q + b]), BatchSim::first / nbx counted in step-kernel tiles.
+cudaError_t launch_batch_tma_fp32(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
+                                  long long total, int stress, int grid, cudaStream_t s);
+cudaError_t launch_batch_tma_fp64(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
+                                  long long total, int stress, int grid, cudaStream_t s);
+// Sets the kernel's shared-memory size and returns its resident blocks per SM
+// (call before any graph capture).
+cudaError_t batch_tma_prepare_fp32(int stress, int* blocks_per_sm);
+cudaError_t batch_tma_prepare_fp64(int stress, int* blocks_per_sm);
 cudaError_t prepare_particles_batch();
 cudaError_t launch_wait_selftest(int* status, uint32_t limit, cudaStream_t s);
 cudaError_t launch_particles_batch(const ParticleArgs* args, int nsim, cudaStream_t s);

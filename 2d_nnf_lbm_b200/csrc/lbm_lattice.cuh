@@ -1034,6 +1034,14 @@ struct TileCand {
   int idx[MAX_TILE_CAND];
   int n;
   int bx, by;  // the tile in this stage
+  // batched step only: the tile's simulation, its buffers and step, and the
+  // slot of the shared ring that holds its LatticeArgs
+  int sim, rslot, aslot, pad;
+  long long step;
+  const void* src;
+  void* dst;
+  const void* om_src;
+  void* om_dst;
 };
 
 template <class T>
@@ -1137,6 +1145,237 @@ __device__ __forceinline__ void cand_copy(const LatticeArgs& a, CandList c, int 
 #ifndef LBM_STEP_MINB_F32
 #define LBM_STEP_MINB_F32 2
 #endif
+
+
+// Per-launch buffers of one simulation's step: the single-run kernel takes
+// them from its arguments, the batched kernel from the stage's simulation.
+template <class T>
+struct StepIO {
+  const T* src;     // f*(k), read by the edge gathers (the boxes come by TMA)
+  T* dst;           // f*(k+1)
+  const T* om_src;  // per-node omega of the Bingham models
+  T* om_dst;
+  long long step;   // the launch's step k
+};
+
+// One node's values between the stage read and the collision.
+template <class T>
+struct NodeVals {
+  T f[9];
+  T rho, drho, ux, uy, gx, gy;
+  Mom32 mq;
+};
+
+// Node (i, j) of a staged tile: populations after streaming and the
+// boundary conditions, macroscopic variables, lattice health, SPM body force
+// (the highest-index disk with PHI > 0 sets G) and the warp's force sums.
+// Every lane of the warp calls it (act: the node is in the lattice; edge:
+// it gathers its populations from global memory); q points at the node's
+// stage elements.  PDL: the force accumulators are touched only after
+// griddepcontrol.wait (the particle kernel that zeroes them may still run).
+template <class T, bool PDL>
+__device__ __forceinline__ void node_gather(const LatticeArgs& a, const StepIO<T>& io,
+                                            const TileCand& C, T* const q, int i, int j,
+                                            bool act, bool edge, int lane, bool& waited,
+                                            NodeVals<T>& v) {
+  constexpr bool F64 = sizeof(T) == 8;
+  using ST = Stage<T>;
+  const Geometry& g = a.g;
+  const Model& m = a.m;
+  const T* __restrict__ src = io.src;
+  // ---- streaming + boundary conditions --------------------------------
+  // Nodes inside the lattice take the streamed values from the stage;
+  // nodes on its edge gather theirs with the boundary conditions.
+  T* const f = v.f;
+  if (!edge) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
+  } else if (act) {
+    if (m.bc == BC_EQUILIBRIUM)
+      edge_equilibrium<T>(a, i, j, (int)((io.step - 1) & 1), f);
+    else
+      pull_bc<T>(src, g, m.bc, i, j, f);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = (T)0;
+  }
+
+  // ---- macroscopic variables (C1:1421-1439) ---------------------------
+  T rho, drho, ux, uy;
+  Mom32& mq = v.mq;
+  if (F64) {
+    rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    drho = rho - (T)m.rho0;
+    const T rinv = (T)1.0 / rho;
+    ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
+    uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
+  } else {
+    float hq[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) hq[k] = (float)f[k];
+    mq = moments32(hq);
+    drho = (T)mq.drho;
+    rho = (T)(m.rho0_f + mq.drho);
+    const float rinv = __fdividef(1.0f, (float)rho);
+    ux = (T)(mq.jx * rinv);
+    uy = (T)(mq.jy * rinv);
+  }
+  if (!act) {
+    rho = (T)1;
+    drho = (T)0;
+    ux = uy = (T)0;
+  }
+  lattice_health<T>(a.status, drho, lane);
+  // FP64 reads f back from the stage after the particle loop instead of
+  // holding 18 registers across it; edge nodes park theirs there first
+  if (F64 && edge && act) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q[ST::off(k)] = f[k];
+  }
+
+  // ---- SPM body force (the highest-index particle with PHI>0 sets G,
+  //      C1:500-507) and force sums ---------------------------------------
+  T gx = (T)0, gy = (T)0;
+  int gbest = -1;
+  // Only the candidates whose disk reaches this warp's 32 nodes of row j
+  // are visited: for the others every node of the segment is at least
+  // R + zeta/2 + 1e-3 from the centre, so PHI is 0 there in either
+  // precision (rounding of the node distance is far below 1e-3) and the
+  // skipped iterations would add nothing.
+  unsigned near = 0;
+  {
+    bool nr = false;
+    if (lane < C.n) {  // the warp's nodes: columns i - lane .. i - lane + 31
+      const double dl = (double)(i - lane) - C.px[lane], dr = dl + 31.0;
+      const double dx = dl > 0.0 ? dl : (dr < 0.0 ? -dr : 0.0);
+      const double dy = (double)j - C.py[lane];
+      const double reach = 0.5 * C.pd[lane] + 0.5 * m.zeta + 1e-3;
+      nr = dx * dx + dy * dy < reach * reach;
+    }
+    near = __ballot_sync(0xffffffffu, nr);
+  }
+  while (near) {
+    const int c = __ffs(near) - 1;
+    near &= near - 1;
+    double fx = 0.0, fy = 0.0, tz = 0.0;
+    bool hit = false;
+    if (act) {
+      const double di = (double)i - C.px[c];
+      const double dj = (double)j - C.py[c];
+      T phi;
+      if (F64)
+        phi = (T)phi_double(di, dj, 0.5 * C.pd[c], m.zeta, m.pi);
+      else
+        phi = (T)phi_float((float)di, (float)dj, (float)(0.5 * C.pd[c]), m.zeta_f, m.pi_f);
+      if (phi > (T)0) {
+        hit = true;
+        const T uxp = (T)C.pu[c] - (T)C.pw[c] * (T)dj;
+        const T uyp = (T)C.pv[c] + (T)C.pw[c] * (T)di;
+        if (C.idx[c] > gbest) {
+          gbest = C.idx[c];
+          gx = phi * (uxp - ux);
+          gy = phi * (uyp - uy);
+        }
+        const T rp = rho * phi;
+        fx = (double)(rp * (ux - uxp));
+        fy = (double)(rp * (uy - uyp));
+        tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
+      }
+    }
+    if (__any_sync(0xffffffffu, hit)) {
+      // warp totals of (Fx, Fy, Tz) in lanes 0, 8, 16
+      const double tot = warp_sum3(fx, fy, tz, lane);
+      if (PDL && !waited) {  // the particle kernel has zeroed the accumulators
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        waited = true;
+      }
+      const int comp = lane >> 3;
+      if ((lane & 7) == 0 && comp < 3) {
+        const long long st = a.npad;
+        unsigned long long* acc = a.facc + C.idx[c] + 2 * comp * st;
+        facc_add(acc, acc + st, tot);
+      }
+    }
+  }
+  if (F64 && act) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
+  }
+  v.rho = rho;
+  v.drho = drho;
+  v.ux = ux;
+  v.uy = uy;
+  v.gx = gx;
+  v.gy = gy;
+}
+
+// Velocity correction and collision of the next step of node (i, j) (row
+// offset nd), then its stores.
+template <class T, bool STRESS>
+__device__ __forceinline__ void node_collide(const LatticeArgs& a, const StepIO<T>& io,
+                                             NodeVals<T>& v, int i, int j, long long nd) {
+  constexpr bool F64 = sizeof(T) == 8;
+  const Model& m = a.m;
+  const long long P = a.g.plane;
+  T* __restrict__ dst = io.dst;
+  // ---- velocity correction (C1:1138-1152) and collision of the next step
+  const T uxc = v.ux + (T)0.5 * (v.gx + (T)0.0);
+  const T uyc = v.uy + (T)0.5 * (v.gy + (T)0.0);
+  if (m.bc == BC_EQUILIBRIUM)
+    ring_store<T>(a, i, j, (int)(io.step & 1), F64 ? v.rho : v.drho, uxc, uyc);
+  const bool want_stress = STRESS;
+  const bool bingham = STRESS && m.bingham;
+  NodeOut no;
+  no.omega = m.omega;
+  no.yield = 0;
+  no.t11 = no.t22 = no.t12 = 0.0;
+  T omn = (T)m.omega;
+  if (bingham) omn = io.om_src[nd];
+  if (F64) {
+    double S[9];
+    if (bingham) {
+      rates_double(m, (double)omn, S);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) S[k] = m.S_uni[k];
+    }
+    double fd[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fd[k] = (double)v.f[k];
+    collide_double(m, fd, (double)v.rho, (double)uxc, (double)uyc, (double)v.gx, (double)v.gy, S,
+                   want_stress, no);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v.f[k] = (T)fd[k];
+  } else {
+    Rates32 r;
+    r.s1 = m.s_e_f;
+    r.s2 = m.s_eps_f;
+    if (bingham) {
+      const float w = (float)omn;
+      r.sw = w;
+      r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : m.sq_uni_f;
+    } else {
+      r.sw = m.omega_f;
+      r.sq = m.sq_uni_f;
+    }
+    float hf[9];
+    relax32(m, v.mq, (float)v.rho, (float)uxc, (float)uyc, (float)v.gx, (float)v.gy, r,
+            want_stress, no, hf);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v.f[k] = (T)hf[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) dst[plane_of(k) * P + nd] = v.f[k];
+  if (bingham) io.om_dst[nd] = (T)no.omega;
+  if (STRESS && m.record_stress) {
+    const int slot = (int)((io.step + 1) & 1);
+    T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * P;
+    rec[nd] = (T)no.t11;
+    rec[P + nd] = (T)no.t22;
+    rec[2 * P + nd] = (T)no.t12;
+    rec[3 * P + nd] = (T)no.yield;
+  }
+}
 
 // STRESS: the model needs the strain rate (Bingham viscosity or recorded
 // stress); the Newtonian instantiation carries none of that code.
@@ -1321,12 +1560,11 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
   }
 
   // ================= consumer warps ========================================
-  const int kpar = (int)(a.step & 1), rslot = a.rec_slot;
+  const int rslot = a.rec_slot;
   bool waited = false;  // griddepcontrol.wait done (before the first force sum)
   const int tr = tid / ST::TW, tc = tid - tr * ST::TW;  // row and column in the tile
-  const T* __restrict__ src = static_cast<const T*>(a.src);
-  T* __restrict__ dst = static_cast<T*>(a.dst);
-  const long long P = g.plane;
+  const StepIO<T> io{static_cast<const T*>(a.src), static_cast<T*>(a.dst),
+                     static_cast<const T*>(a.om_src), static_cast<T*>(a.om_dst), a.step};
   const int pt = g.pitch;
   int sidx = 0;
   uint32_t fpar = 0;  // per-stage parity of the next "full" completion
@@ -1356,198 +1594,23 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       continue;
     }
     const TileCand& C = cands[sidx];
-
-    // ---- streaming + boundary conditions --------------------------------
-    // Nodes inside the lattice take the streamed values from the stage;
-    // nodes on its edge gather theirs with the boundary conditions.
     const bool act = (i <= g.nx) && (j <= g.ny);
     const bool edge = (i == 0) || (i >= g.nx) || (j == 0) || (j >= g.ny);
-    T f[9];
     // this node's nine stage elements: planes in plane_of order, the row
-    // shift is in the box, the column shift -c_x is applied here.  Pull
+    // shift is in the box, the column shift -c_x is applied in ST::off.  Pull
     // streaming is a bijection, so no other node reads these elements.
     T* const q = stage_w + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
-    if (!edge) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
-    } else if (act) {
-      if (m.bc == BC_EQUILIBRIUM)
-        edge_equilibrium<T>(a, i, j, (int)((a.step - 1) & 1), f);
-      else
-        pull_bc<T>(src, g, m.bc, i, j, f);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = (T)0;
-    }
-
-    // ---- macroscopic variables (C1:1421-1439) ---------------------------
-    T rho, drho, ux, uy;
-    Mom32 mq;
-    if (F64) {
-      rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-      drho = rho - (T)m.rho0;
-      const T rinv = (T)1.0 / rho;
-      ux = rinv * (f[1] + f[5] + f[8] - (f[6] + f[3] + f[7]));
-      uy = rinv * (f[5] + f[2] + f[6] - (f[7] + f[4] + f[8]));
-    } else {
-      float hq[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) hq[k] = (float)f[k];
-      mq = moments32(hq);
-      drho = (T)mq.drho;
-      rho = (T)(m.rho0_f + mq.drho);
-      const float rinv = __fdividef(1.0f, (float)rho);
-      ux = (T)(mq.jx * rinv);
-      uy = (T)(mq.jy * rinv);
-    }
-    if (!act) {
-      rho = (T)1;
-      drho = (T)0;
-      ux = uy = (T)0;
-    }
-    lattice_health<T>(a.status, drho, lane);
-    // FP64 reads f back from the stage after the particle loop instead of
-    // holding 18 registers across it; edge nodes park theirs there first
-    if (F64 && edge && act) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) q[ST::off(k)] = f[k];
-    }
-
-    // ---- SPM body force (the highest-index particle with PHI>0 sets G,
-    //      C1:500-507) and force sums ---------------------------------------
-    T gx = (T)0, gy = (T)0;
-    int gbest = -1;
-    // Only the candidates whose disk reaches this warp's 32 nodes of row j
-    // are visited: for the others every node of the segment is at least
-    // R + zeta/2 + 1e-3 from the centre, so PHI is 0 there in either
-    // precision (rounding of the node distance is far below 1e-3) and the
-    // skipped iterations would add nothing.
-    unsigned near = 0;
-    {
-      bool nr = false;
-      if (lane < C.n) {  // the warp's nodes: columns i - lane .. i - lane + 31
-        const double dl = (double)(i - lane) - C.px[lane], dr = dl + 31.0;
-        const double dx = dl > 0.0 ? dl : (dr < 0.0 ? -dr : 0.0);
-        const double dy = (double)j - C.py[lane];
-        const double reach = 0.5 * C.pd[lane] + 0.5 * m.zeta + 1e-3;
-        nr = dx * dx + dy * dy < reach * reach;
-      }
-      near = __ballot_sync(0xffffffffu, nr);
-    }
-    while (near) {
-      const int c = __ffs(near) - 1;
-      near &= near - 1;
-      double fx = 0.0, fy = 0.0, tz = 0.0;
-      bool hit = false;
-      if (act) {
-        const double di = (double)i - C.px[c];
-        const double dj = (double)j - C.py[c];
-        T phi;
-        if (F64)
-          phi = (T)phi_double(di, dj, 0.5 * C.pd[c], m.zeta, m.pi);
-        else
-          phi = (T)phi_float((float)di, (float)dj, (float)(0.5 * C.pd[c]), m.zeta_f, m.pi_f);
-        if (phi > (T)0) {
-          hit = true;
-          const T uxp = (T)C.pu[c] - (T)C.pw[c] * (T)dj;
-          const T uyp = (T)C.pv[c] + (T)C.pw[c] * (T)di;
-          if (C.idx[c] > gbest) {
-            gbest = C.idx[c];
-            gx = phi * (uxp - ux);
-            gy = phi * (uyp - uy);
-          }
-          const T rp = rho * phi;
-          fx = (double)(rp * (ux - uxp));
-          fy = (double)(rp * (uy - uyp));
-          tz = (double)(rp * ((T)di * (uy - uyp) - (T)dj * (ux - uxp)));
-        }
-      }
-      if (__any_sync(0xffffffffu, hit)) {
-        // warp totals of (Fx, Fy, Tz) in lanes 0, 8, 16
-        const double tot = warp_sum3(fx, fy, tz, lane);
-        if (!waited) {  // the particle kernel has zeroed the accumulators
-          asm volatile("griddepcontrol.wait;" ::: "memory");
-          waited = true;
-        }
-        const int q = lane >> 3;
-        if ((lane & 7) == 0 && q < 3) {
-          const long long st = a.npad;
-          unsigned long long* acc = a.facc + C.idx[c] + 2 * q * st;
-          facc_add(acc, acc + st, tot);
-        }
-      }
-    }
-    if (F64 && act) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = q[ST::off(k)];
-    }
+    NodeVals<T> v;
+    node_gather<T, true>(a, io, C, q, i, j, act, edge, lane, waited, v);
     // the stage and its candidates are consumed
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
 
     // ---- mean density at history steps (C1:318): fixed-point, order-free -
     if (rslot >= 0 && act)
-      mass_q += F64 ? __double2ll_rn((double)drho * MASS_FIX)
-                    : mass_share32((float)drho);
-    if (!act) continue;
-
-    // ---- velocity correction (C1:1138-1152) and collision of the next step
-    const T uxc = ux + (T)0.5 * (gx + (T)0.0);
-    const T uyc = uy + (T)0.5 * (gy + (T)0.0);
-    if (m.bc == BC_EQUILIBRIUM)
-      ring_store<T>(a, i, j, (int)(a.step & 1), F64 ? rho : drho, uxc, uyc);
-    const bool want_stress = STRESS;
-    const bool bingham = STRESS && m.bingham;
-    NodeOut no;
-    no.omega = m.omega;
-    no.yield = 0;
-    no.t11 = no.t22 = no.t12 = 0.0;
-    T omn = (T)m.omega;
-    if (bingham) omn = static_cast<const T*>(a.om_src)[nd];
-    if (F64) {
-      double S[9];
-      if (bingham) {
-        rates_double(m, (double)omn, S);
-      } else {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) S[k] = m.S_uni[k];
-      }
-      double fd[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) fd[k] = (double)f[k];
-      collide_double(m, fd, (double)rho, (double)uxc, (double)uyc, (double)gx, (double)gy, S,
-                     want_stress, no);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = (T)fd[k];
-    } else {
-      Rates32 r;
-      r.s1 = m.s_e_f;
-      r.s2 = m.s_eps_f;
-      if (bingham) {
-        const float w = (float)omn;
-        r.sw = w;
-        r.sq = m.q_of_omega ? 8.0f * (2.0f - w) / (8.0f - w) : m.sq_uni_f;
-      } else {
-        r.sw = m.omega_f;
-        r.sq = m.sq_uni_f;
-      }
-      float hf[9];
-      relax32(m, mq, (float)rho, (float)uxc, (float)uyc, (float)gx, (float)gy, r, want_stress, no,
-              hf);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) f[k] = (T)hf[k];
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) dst[plane_of(k) * P + nd] = f[k];
-    if (bingham) static_cast<T*>(a.om_dst)[nd] = (T)no.omega;
-    if (STRESS && m.record_stress) {
-      const int slot = (kpar + 1) & 1;
-      T* rec = static_cast<T*>(a.rec) + (long long)slot * 4 * P;
-      rec[nd] = (T)no.t11;
-      rec[P + nd] = (T)no.t22;
-      rec[2 * P + nd] = (T)no.t12;
-      rec[3 * P + nd] = (T)no.yield;
-    }
+      mass_q += F64 ? __double2ll_rn((double)v.drho * MASS_FIX)
+                    : mass_share32((float)v.drho);
+    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd);
   }
   if (rslot >= 0) {
 #pragma unroll
@@ -1606,6 +1669,267 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kern, a, *tm);
+}
+
+// ---------------------------------------------------------------------------
+// Batched step on the TMA pipeline: the warp-specialised step of k_step over
+// the tiles of every simulation of a batch (MRT models; a batch with a BGK
+// run takes the one-node-per-thread kernel below).  Tiles are numbered
+// simulation by simulation (row-major inside one, BatchSim::first), and
+// block b takes a contiguous range of them, so it stays in one or two
+// simulations.  Entering a simulation, the producer reads its device
+// counters (step number, ping-pong buffer, history slot, list buffer: a
+// captured graph replays unchanged) and picks the tensor map of that buffer
+// (two per simulation, in global memory).  Per tile it issues the boxes,
+// stages the candidates and notes the tile's simulation, buffers and step in
+// the stage; the simulation's LatticeArgs go into a slot of a small shared
+// ring that the consumers read their model from.  A slot is rewritten only
+// after every consumer warp has finished the tile that used it (warps are at
+// most NSTAGE tiles apart, the ring holds 2 NSTAGE).  The node arithmetic is
+// k_step's (node_gather, node_collide).  Launches do not overlap: the
+// batched particle kernel runs between two.
+constexpr int BATCH_ARGS_SLOTS = 2 * NSTAGE;
+
+template <class T>
+constexpr int batch_step_smem() {
+  return step_smem<T>() + BATCH_ARGS_SLOTS * (int)sizeof(LatticeArgs);
+}
+
+template <class T, bool STRESS>
+__global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F32)
+    k_step_batch(const BatchSim* __restrict__ sims, int nsim,
+                 const CUtensorMap* __restrict__ tmaps, long long total) {
+  constexpr bool F64 = sizeof(T) == 8;
+  constexpr uint32_t WAIT = 1u << 20;
+  using ST = Stage<T>;
+  static_assert(sizeof(LatticeArgs) % 8 == 0 && sizeof(TileCand) % 8 == 0, "8-byte words");
+  extern __shared__ __align__(128) unsigned char s_raw[];
+  T* const stage_w = reinterpret_cast<T*>(s_raw);
+  const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(s_raw);
+  const uint32_t full0 = s_base + NSTAGE * ST::BYTES;
+  const uint32_t empty0 = full0 + 8 * NSTAGE;
+  unsigned char* const cand_raw = s_raw + NSTAGE * ST::BYTES + 16 * NSTAGE + 64;
+  TileCand* cands = reinterpret_cast<TileCand*>(cand_raw);
+  LatticeArgs* ring = reinterpret_cast<LatticeArgs*>(cand_raw + NSTAGE * sizeof(TileCand));
+  __shared__ int s_ring_sim[BATCH_ARGS_SLOTS];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  if (tid < BATCH_ARGS_SLOTS) s_ring_sim[tid] = -1;
+  if (tid == 0) {
+    for (int st = 0; st < NSTAGE; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(full0 + 8 * st) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0 + 8 * st),
+                   "r"(STEP_CONSUMERS / 32)
+                   : "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  const long long t_lo = (long long)blockIdx.x * per;
+  const long long t_hi = t_lo + per < total ? t_lo + per : total;
+
+  if (warp == STEP_CONSUMERS / 32) {
+    // ================= producer warp =====================================
+    int q = 0;
+    if (lane == 0) {  // the last simulation whose first tile is <= t_lo
+      int lo = 0, hi = nsim - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sims[mid].first <= t_lo) lo = mid;
+        else hi = mid - 1;
+      }
+      q = lo;
+    }
+    q = __shfl_sync(0xffffffffu, q, 0);
+    // the simulation being staged, from its device counters
+    long long first = 0, next = 0, kk = 0;
+    int ntx = 1, ltx = 1, nx = 0, buf = 0, lbuf = 0, rslot = -1;
+    const CUtensorMap* tm = nullptr;
+    auto enter = [&](int sq) {
+      const BatchSim& B = sims[sq];
+      long long k = 0, f0 = 0, f1 = 0;
+      int b = 0, lb = 0, rs = -1;
+      if (lane == 0) {
+        k = *B.kk;
+        b = (int)((B.par0 + k - 1) & 1);
+        rs = *B.rec_slot;
+        lb = B.a.tile_cur[k & 1];
+        f0 = B.first;
+        f1 = sq + 1 < nsim ? sims[sq + 1].first : total;
+      }
+      kk = __shfl_sync(0xffffffffu, k, 0);
+      buf = __shfl_sync(0xffffffffu, b, 0);
+      rslot = __shfl_sync(0xffffffffu, rs, 0);
+      lbuf = __shfl_sync(0xffffffffu, lb, 0);
+      first = __shfl_sync(0xffffffffu, f0, 0);
+      next = __shfl_sync(0xffffffffu, f1, 0);
+      ntx = B.nbx;
+      ltx = B.a.g.ltx;
+      nx = B.a.g.nx;
+      tm = tmaps + 2 * sq + buf;
+    };
+    if (t_lo < t_hi) enter(q);
+    int sidx = 0, n = 0;
+    uint32_t epar = 0, fpar = 0;
+    bool alive = true;
+    for (long long t = t_lo; t < t_hi; ++t) {
+      while (t >= next) enter(++q);
+      const BatchSim& B = sims[q];
+      const int local = (int)(t - first);
+      const int by = local / ntx, bx = local - by * ntx;
+      const CandList cl =
+          cand_list(B.a, ((by * ST::TR) / LTY) * ltx + (bx * ST::TW) / LTX, lbuf, lane);
+      if (n >= NSTAGE) {
+        bool ok = true;
+        if (lane == 0) {
+          ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+          if (!ok) atomicOr(B.a.status, ST_TIMEOUT);
+        }
+        epar ^= 1u << sidx;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) {
+            for (int st = 0; st < NSTAGE; ++st)
+              mbar_wait(full0 + 8 * st, ((fpar >> st) & 1u) ^ 1u, WAIT);
+          }
+          alive = false;
+          break;
+        }
+      }
+      // the simulation's arguments into the ring slot of this tile
+      const int slot = n % BATCH_ARGS_SLOTS;
+      if (s_ring_sim[slot] != q) {
+        const unsigned long long* from = reinterpret_cast<const unsigned long long*>(&B.a);
+        unsigned long long* to = reinterpret_cast<unsigned long long*>(&ring[slot]);
+        for (int w = lane; w < (int)(sizeof(LatticeArgs) / 8); w += 32) to[w] = from[w];
+        __syncwarp();
+        if (lane == 0) s_ring_sim[slot] = q;
+      }
+      TileCand& C = cands[sidx];
+      const uint32_t fb = full0 + 8 * sidx;
+      if (lane == 0) {
+        C.sim = q;
+        C.rslot = rslot;
+        C.aslot = slot;
+        C.step = kk;
+        C.src = B.f[buf];
+        C.dst = B.f[buf ^ 1];
+        C.om_src = B.om[buf];
+        C.om_dst = B.om[buf ^ 1];
+        if (bx * ST::TW >= nx) {
+          mbar_arrive(fb);  // every node on the right edge gathers from global memory
+        } else {
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
+                       "r"((uint32_t)ST::BYTES)
+                       : "memory");
+          tma_tile<T>(tm, s_base + sidx * ST::BYTES, fb, bx, by);
+        }
+      }
+      cand_copy(B.a, cl, bx, by, C, lane, fb);
+      fpar ^= 1u << sidx;
+      sidx = sidx + 1 == NSTAGE ? 0 : sidx + 1;
+      ++n;
+    }
+    if (alive) {
+      bool ok = true;
+      if (lane == 0) {
+        if (n >= NSTAGE) ok = mbar_wait(empty0 + 8 * sidx, (epar >> sidx) & 1u, WAIT);
+        if (ok) {
+          cands[sidx].bx = -1;
+          mbar_arrive(full0 + 8 * sidx);
+          mbar_arrive(full0 + 8 * sidx);
+        }
+      }
+    }
+    return;
+  }
+
+  // ================= consumer warps ========================================
+  bool waited = true;  // no programmatic dependence: the particles are done
+  const int tr = tid / ST::TW, tc = tid - tr * ST::TW;
+  int sidx = 0;
+  uint32_t fpar = 0;
+  // the warp's mean-density share of the current simulation's history slot,
+  // added when the warp moves to another simulation or leaves
+  long long mass_q = 0;
+  int cur = -1, cur_rslot = -1;
+  unsigned long long* cur_mass = nullptr;
+  auto flush_mass = [&]() {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mass_q += __shfl_down_sync(0xffffffffu, mass_q, o);
+    if (lane == 0 && mass_q != 0 && cur_mass && cur_rslot >= 0)
+      atomicAdd(cur_mass + cur_rslot, (unsigned long long)mass_q);
+    mass_q = 0;
+  };
+  for (;; sidx = (sidx + 1 == NSTAGE ? 0 : sidx + 1)) {
+    if (!mbar_wait(full0 + 8 * sidx, (fpar >> sidx) & 1u, WAIT)) {
+      // the producer wrote no status word for a stage it never filled: the
+      // current simulation's (or the first one's) takes the timeout
+      if (lane == 0) atomicOr(sims[cur >= 0 ? cur : 0].a.status, ST_TIMEOUT);
+      return;
+    }
+    fpar ^= 1u << sidx;
+    const TileCand& C = cands[sidx];
+    const int bx = C.bx, by = C.by;
+    if (bx < 0) break;
+    const LatticeArgs& a = ring[C.aslot];
+    if (C.sim != cur) {
+      flush_mass();
+      cur = C.sim;
+      cur_rslot = C.rslot;
+      cur_mass = a.mass_acc;
+    }
+    const Geometry& g = a.g;
+    const StepIO<T> io{static_cast<const T*>(C.src), static_cast<T*>(C.dst),
+                       static_cast<const T*>(C.om_src), static_cast<T*>(C.om_dst), C.step};
+    const int i = bx * ST::TW + tc;
+    const int j = by * ST::TR + tr;
+    const long long nd = (long long)j * g.pitch + i;
+    const bool warp_live = (j <= g.ny) && (bx * ST::TW + (tc & ~31) <= g.nx);
+    if (!warp_live) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
+      continue;
+    }
+    const bool act = (i <= g.nx) && (j <= g.ny);
+    const bool edge = (i == 0) || (i >= g.nx) || (j == 0) || (j >= g.ny);
+    T* const qp = stage_w + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
+    NodeVals<T> v;
+    node_gather<T, false>(a, io, C, qp, i, j, act, edge, lane, waited, v);
+    // the stage and its candidates are consumed (the ring slot is not)
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
+    if (cur_rslot >= 0 && cur_mass != nullptr && act)
+      mass_q += F64 ? __double2ll_rn((double)v.drho * MASS_FIX) : mass_share32((float)v.drho);
+    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd);
+  }
+  flush_mass();
+}
+
+template <class T>
+cudaError_t batch_tma_prepare(int stress, int* blocks_per_sm) {
+  constexpr int SMEM = batch_step_smem<T>();
+  void (*const kern)(const BatchSim*, int, const CUtensorMap*, long long) =
+      stress ? k_step_batch<T, true> : k_step_batch<T, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, STEP_TPB, SMEM);
+}
+
+template <class T>
+cudaError_t launch_batch_tma(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
+                             long long total, int stress, int grid, cudaStream_t s) {
+  constexpr int SMEM = batch_step_smem<T>();
+  if (stress)
+    k_step_batch<T, true><<<grid, STEP_TPB, SMEM, s>>>(sims, nsim, tmaps, total);
+  else
+    k_step_batch<T, false><<<grid, STEP_TPB, SMEM, s>>>(sims, nsim, tmaps, total);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -354,12 +354,16 @@ def trajectory_error(pkg, args, device, steps):
         r32, r64 = sims[1].particles(), sims[0].particles()
         d32, d64 = r32[:, 0:2] - pin[:, 0:2], r64[:, 0:2] - pin[:, 0:2]
         v32, v64 = r32[:, 3:5], r64[:, 3:5]
+        dmax = max(float(np.max(np.linalg.norm(d64, axis=1))), tiny)
+        vmax = max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)
+        ed = np.linalg.norm(d32 - d64, axis=1) / dmax
+        ev = np.linalg.norm(v32 - v64, axis=1) / vmax
         at.append({
             "steps": m,
-            "max_rel_displacement_err": float(np.max(np.linalg.norm(d32 - d64, axis=1)) /
-                                              max(float(np.max(np.linalg.norm(d64, axis=1))), tiny)),
-            "max_rel_velocity_err": float(np.max(np.linalg.norm(v32 - v64, axis=1)) /
-                                          max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)),
+            "max_rel_displacement_err": float(ed.max()),
+            "rms_rel_displacement_err": float(np.sqrt(np.mean(ed ** 2))),
+            "max_rel_velocity_err": float(ev.max()),
+            "rms_rel_velocity_err": float(np.sqrt(np.mean(ev ** 2))),
             "max_fp64_displacement": float(np.max(np.linalg.norm(d64, axis=1))),
             "status": [sims[1].status(), sims[0].status()],
         })
@@ -369,7 +373,9 @@ def trajectory_error(pkg, args, device, steps):
     return {
         "steps": steps,
         "max_rel_displacement_err": last["max_rel_displacement_err"],
+        "rms_rel_displacement_err": last["rms_rel_displacement_err"],
         "max_rel_velocity_err": last["max_rel_velocity_err"],
+        "errors_relative_to": "the largest FP64 displacement (speed) over all disks",
         "tolerance": 1e-4,
         "within_tolerance": bool(last["max_rel_displacement_err"] <= 1e-4 and
                                  last["max_rel_velocity_err"] <= 1e-4),
@@ -514,14 +520,18 @@ def adjoint_measure(pkg, torch, device):
         sim.close()
         return float(np.mean(v))
 
-    fd = {}
+    # central differences: parameters at a relative step of 1e-4; the
+    # release point at 1e-4 of the disk diameter (a step relative to the
+    # coordinate itself, 0.1 lu at y0 = 1032, would measure how the disk
+    # sits on the lattice, not the derivative), and again at half that step
+    fd, fd_half = {}, {}
     names = ("tau_y", "nu", "rho_p", "x0", "y0")
     col = {"rho_p": 7, "x0": 0, "y0": 1}
-    for name in names:
+
+    def central(name, d):
         base = {"tau_y": p64.tau_y, "nu": p64.nu}.get(name, None)
         if base is None:
             base = float(pin[0, col[name]])
-        d = 1e-4 * abs(base)
         jj = []
         for sgn in (1.0, -1.0):
             q = p64.copy()
@@ -533,7 +543,16 @@ def adjoint_measure(pkg, torch, device):
             else:
                 disks[0, col[name]] = base + sgn * d
             jj.append(run_j(q, disks))
-        fd[name] = (jj[0] - jj[1]) / (2 * d)
+        return (jj[0] - jj[1]) / (2 * d)
+
+    for name in names:
+        if name in ("x0", "y0"):
+            d = 1e-4 * float(pin[0, 6])
+            fd[name] = central(name, d)
+            fd_half[name] = central(name, 0.5 * d)
+        else:
+            base = {"tau_y": p64.tau_y, "nu": p64.nu, "rho_p": float(pin[0, 7])}[name]
+            fd[name] = central(name, 1e-4 * abs(base))
     j32, g32 = res[1]
     j64, g64 = res[0]
     pick = lambda g, k: float(g[k] if k in ("tau_y", "nu") else g[k][0])  # noqa: E731
@@ -549,7 +568,8 @@ def adjoint_measure(pkg, torch, device):
         "grad_fp32": {k: pick(g32, k) for k in fd},
         "grad_fp64": {k: pick(g64, k) for k in fd},
         "fd_fp64": fd,
-        "fd_rel_step": 1e-4,
+        "fd_fp64_half_step": fd_half,
+        "fd_step": "1e-4 relative (tau_y, nu, rho_p); 1e-4 * D for x0, y0",
         "max_rel_err_fp32_vs_fd": max(abs(pick(g32, k) - fd[k]) / abs(fd[k]) for k in rel),
         "max_rel_err_fp64_vs_fd": max(abs(pick(g64, k) - fd[k]) / abs(fd[k]) for k in rel),
         "max_rel_err_fp32_vs_fp64_adjoint": max(abs(pick(g32, k) - pick(g64, k)) /

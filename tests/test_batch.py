@@ -133,13 +133,14 @@ def test_batch_rejects_mixed_precision(pkg, cases):
         b.set_tuning(48, 4, 2)
 
 
+@pytest.mark.parametrize("tma", [False, True])
 @pytest.mark.parametrize("precision,rtol", [(0, 1e-10), (1, 1e-4)])
-def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol):
-    """Each MRT run of a batch (the batched kernel's one-node-per-thread tile
-    body) against the oracle's run of the same inputs, not against another
-    GPU path: the C6 Bingham case (the GPU's per-node omega, oracle rule
-    omega_chain=0, 1e-8 in FP64 as in the single-run parity tests), C1
-    Zou-He and a C3 pair in contact range."""
+def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol, tma):
+    """Each MRT run of a batch (the one-node-per-thread kernel at 32 x 8
+    tiles, or the TMA-staged kernel) against the oracle's run of the same
+    inputs, not against another GPU path: the C6 Bingham case (the GPU's
+    per-node omega, oracle rule omega_chain=0, 1e-8 in FP64 as in the
+    single-run parity tests), C1 Zou-He and a C3 pair in contact range."""
     from oracle.oracle import Oracle
 
     cs = []
@@ -150,6 +151,7 @@ def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol):
         cs.append((name, p, pin))
     steps = 41
     b = pkg.Batch([p for _, p, _ in cs])
+    b.set_tuning(*(_tma_shape(precision) if tma else (32, 8, 4)))
     for s, (_, _, pin) in zip(b.sims, cs):
         s.set_particles(pin)
     b.step(steps)
@@ -171,3 +173,53 @@ def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol):
             assert np.max(np.abs(g - r)) <= tol * max(sc, 1e-300), (name, fld)
         ref.close()
     b.close()
+
+
+def _tma_shape(precision):
+    return (64, 8, 1) if precision == 0 else (128, 4, 2)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_tma_tiles_match_each_simulation_alone(pkg, cases, precision):
+    """The TMA-staged batched kernel (k_step_batch: the single-run step
+    kernel's tiles and node arithmetic over every simulation of the batch)
+    against each run alone through lbm_step: bit for bit in FP64, within
+    1e-6 in FP32; MRT runs only (Bingham, Zou-He, a pair, odd sizes, the
+    equilibrium boundary with prescribed motion, no disks)."""
+    cs = mixed_cases(cases, precision)[:6]
+    steps = 29
+    ref = [run_alone(pkg, p, pin, steps) for p, pin in cs]
+    b = pkg.Batch([p for p, _ in cs])
+    shape = _tma_shape(precision)
+    b.set_tuning(*shape)
+    for s, (_, pin) in zip(b.sims, cs):
+        if pin is not None:
+            s.set_particles(pin)
+    b.step(11)
+    b.step(steps - 11)
+    assert b.tuning()[:2] == shape[:2]
+    for q, s in enumerate(b.sims):
+        if precision == 0:
+            assert_same(state(s), ref[q], ("tma", q))
+        else:
+            assert_close(state(s), ref[q], ("tma", q))
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_tma_tiles_agree_with_scalar_tiles(pkg, cases, precision):
+    cs = mixed_cases(cases, precision)[:4]
+    ref = batch_run(pkg, cs, (32, 8, 2), 24)
+    b = pkg.Batch([p for p, _ in cs])
+    shape = _tma_shape(precision)
+    b.set_tuning(*shape)
+    for s, (_, pin) in zip(b.sims, cs):
+        s.set_particles(pin)
+    b.step(24)
+    got = [state(s) for s in b.sims]
+    b.close()
+    for q in range(len(cs)):
+        if precision == 0:
+            assert_same(got[q], ref[q], ("tma-vs-scalar", q))
+        else:
+            assert_close(got[q], ref[q], ("tma-vs-scalar", q))

@@ -11,8 +11,7 @@ the previous step (oracle rule omega_chain=0).  On the C6 program at 40 x
   the terminal v_y of the two rules differ by about 26 % and about 1.6 % of
   the fluid nodes carry a different yield flag at the end.  The difference
   is the chain's one-node shift of the yield surface: it is about 15 % at
-  L_C = 20 (tests/golden/omega_chain_study.py) and falls further with
-  resolution.
+  L_C = 20 and 3 % at L_C = 40 (tests/golden/omega_chain_study.py).
   yield number 0.5 (the disk is held by the yield stress): below 0.1 %, no
   flag differs.
 
