@@ -26,7 +26,8 @@
 using namespace lbm;
 
 struct lbm_sim {
-  CUtensorMap tm[2];  // TMA descriptors of f[0], f[1] for the step kernel
+  CUtensorMap tm[2];   // TMA descriptors of f[0], f[1] for the step kernel
+  CUtensorMap tmo[2];  // and of om[0], om[1] (Bingham models; else copies of tm)
   lbm_params p;
   cudaStream_t stream = nullptr;
   Geometry g{};
@@ -110,6 +111,7 @@ struct lbm_sim {
   unsigned char* adj_slots = nullptr;  // [nslots][10 planes]: f*(n) then omega(n)
   int adj_nslots = 0;
   std::vector<CUtensorMap> adj_tm;     // TMA descriptor of each slot's f*
+  std::vector<CUtensorMap> adj_tmo;    // and of its omega plane
   unsigned char* adj_ck = nullptr;     // [nck][10 planes] checkpoints
   int adj_nck = 0;
   double* adj_ckp = nullptr;           // [nck+1][ckp_len]: records, FORCE sums, D_PW
@@ -290,14 +292,14 @@ cudaError_t launch_lattice(lbm_sim* h, const LatticeArgs& a, int mode) {
                                : launch_bgk_step_fp32(a, h->stream);
   if (h->prec == LBM_FP64) {
     switch (mode) {
-      case 0: return launch_step_fp64(a, &h->tm[h->cur], h->stream);
+      case 0: return launch_step_fp64(a, &h->tm[h->cur], &h->tmo[h->cur], h->stream);
       case 1: return launch_output_fp64(a, h->stream);
       case 2: return launch_init_fp64(a, h->stream);
       default: return launch_restart_fp64(a, h->stream);
     }
   }
   switch (mode) {
-    case 0: return launch_step_fp32(a, &h->tm[h->cur], h->stream);
+    case 0: return launch_step_fp32(a, &h->tm[h->cur], &h->tmo[h->cur], h->stream);
     case 1: return launch_output_fp32(a, h->stream);
     case 2: return launch_init_fp32(a, h->stream);
     default: return launch_restart_fp32(a, h->stream);
@@ -659,8 +661,9 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// TMA descriptor of the step kernel's reads from the population buffer at base.
-int encode_f_map(const lbm_sim* h, void* base, CUtensorMap* out) {
+// TMA descriptor of the step kernel's reads from the population buffer at base;
+// tw x rows nodes per tile (default: the single-run step kernel's tile).
+int encode_f_map(const lbm_sim* h, void* base, CUtensorMap* out, int tw = 0, int rows = 0) {
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
@@ -671,11 +674,35 @@ int encode_f_map(const lbm_sim* h, void* base, CUtensorMap* out) {
   const cuuint64_t dims[3] = {(cuuint64_t)h->g.pitch, (cuuint64_t)(h->p.ny + 1), 9};
   const cuuint64_t strides[2] = {(cuuint64_t)h->g.pitch * h->esz,
                                  (cuuint64_t)h->g.plane * h->esz};
-  const cuuint32_t box[3] = {(cuuint32_t)step_box_width((int)h->esz),
-                             (cuuint32_t)step_box_rows((int)h->esz), 3};
+  if (tw <= 0) tw = step_tile_width((int)h->esz);
+  if (rows <= 0) rows = step_box_rows((int)h->esz);
+  const cuuint32_t box[3] = {(cuuint32_t)(tw + 2 * (16 / (int)h->esz)), (cuuint32_t)rows, 3};
   const cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(out, h->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                    3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LBM_OK : LBM_E_CUDA;
+}
+
+// TMA descriptor of the step kernel's reads of the node omega at base (one
+// plane): 2-D, box = one tile (TW nodes x TR rows), no halo.
+int encode_om_map(const lbm_sim* h, void* base, CUtensorMap* out, int tw = 0, int rows = 0) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      fn == nullptr || q != cudaDriverEntryPointSuccess)
+    return LBM_E_CUDA;
+  EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
+  const cuuint64_t dims[2] = {(cuuint64_t)h->g.pitch, (cuuint64_t)(h->p.ny + 1)};
+  const cuuint64_t strides[1] = {(cuuint64_t)h->g.pitch * h->esz};
+  if (tw <= 0) tw = step_tile_width((int)h->esz);
+  if (rows <= 0) rows = step_box_rows((int)h->esz);
+  const cuuint32_t box[2] = {(cuuint32_t)tw, (cuuint32_t)rows};
+  const cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(out, h->esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                   2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? LBM_OK : LBM_E_CUDA;
@@ -685,6 +712,8 @@ int make_tensor_maps(lbm_sim* h) {
   for (int b = 0; b < 2; ++b) {
     int rc = encode_f_map(h, h->f[b], &h->tm[b]);
     if (rc) return rc;
+    h->tmo[b] = h->tm[b];
+    if (h->om[b] && (rc = encode_om_map(h, h->om[b], &h->tmo[b]))) return rc;
   }
   return LBM_OK;
 }
@@ -1469,8 +1498,15 @@ int adj_reserve(lbm_sim* h, int nslots, int nck, long long nhist) {
     h->adj_nslots = 0;
     if ((rc = dalloc(&h->adj_slots, sb * nslots))) return rc;
     h->adj_tm.assign(nslots, CUtensorMap{});
-    for (int s = 0; s < nslots; ++s)
+    h->adj_tmo.assign(nslots, CUtensorMap{});
+    const size_t pb = (size_t)h->g.plane * h->esz;
+    for (int s = 0; s < nslots; ++s) {
       if ((rc = encode_f_map(h, h->adj_slots + sb * s, &h->adj_tm[s]))) return rc;
+      h->adj_tmo[s] = h->adj_tm[s];
+      if (h->m.bingham &&
+          (rc = encode_om_map(h, h->adj_slots + sb * s + 9 * pb, &h->adj_tmo[s])))
+        return rc;
+    }
     h->adj_nslots = nslots;
   }
   if (nck > h->adj_nck || h->adj_npad != h->npad) {
@@ -1561,8 +1597,8 @@ int adj_step_slots(lbm_sim* h, int s) {
   a.dst = dst;
   a.om_src = src + 9 * pb;
   a.om_dst = dst + 9 * pb;
-  if (h->prec == LBM_FP64) CK(launch_step_fp64(a, &h->adj_tm[s], h->stream));
-  else CK(launch_step_fp32(a, &h->adj_tm[s], h->stream));
+  if (h->prec == LBM_FP64) CK(launch_step_fp64(a, &h->adj_tm[s], &h->adj_tmo[s], h->stream));
+  else CK(launch_step_fp32(a, &h->adj_tm[s], &h->adj_tmo[s], h->stream));
   h->partials_valid = true;
   return LBM_OK;
 }
@@ -1809,7 +1845,7 @@ struct lbm_batch {
   int bgk = 0;             // some simulation uses the BGK collision
   int stress = 0;          // some simulation needs the strain rate (TMA kernel variant)
   int tma_bpsm = 0;        // resident blocks per SM of the TMA-staged kernel (0: not usable)
-  CUtensorMap* d_tmaps = nullptr;  // [2 nsim]: each simulation's f[0], f[1]
+  CUtensorMap* d_tmaps = nullptr;  // [4 nsim]: each simulation's f[0], f[1], om[0], om[1]
   int nsm = 148;
   cudaStream_t stream = nullptr;
   BatchSim* d_sims = nullptr;
@@ -1837,12 +1873,11 @@ int batch_grid(const lbm_batch* b) {
 
 // Per-simulation arguments at tile shape `shape`, uploaded to the device.
 // Tile width and height of shape (the TMA shape's depend on the precision).
-int batch_tile_x(const lbm_batch* b, int shape) {
-  return shape == BATCH_SHAPE_TMA ? step_tile_width(b->prec == LBM_FP64 ? 8 : 4)
-                                  : batch_bx(shape);
+int batch_tile_x(const lbm_batch*, int shape) {
+  return shape == BATCH_SHAPE_TMA ? BATCH_TMA_TW : batch_bx(shape);
 }
-int batch_tile_y(const lbm_batch* b, int shape) {
-  return shape == BATCH_SHAPE_TMA ? step_box_rows(b->prec == LBM_FP64 ? 8 : 4) : batch_by(shape);
+int batch_tile_y(const lbm_batch*, int shape) {
+  return shape == BATCH_SHAPE_TMA ? BATCH_TMA_TR : batch_by(shape);
 }
 
 int batch_upload(lbm_batch* b, int shape) {
@@ -2000,10 +2035,17 @@ int lbm_batch_create(const lbm_params* params, int32_t nsim, lbm_batch** out) {
   // (which also sets its shared-memory size, before any graph capture)
   for (lbm_sim* h : b->sims) b->stress |= (h->m.bingham || h->m.record_stress) ? 1 : 0;
   if (!b->bgk) {
-    std::vector<CUtensorMap> tm(2 * (size_t)nsim);
+    std::vector<CUtensorMap> tm(4 * (size_t)nsim);
     for (int q = 0; q < nsim; ++q) {
-      tm[2 * (size_t)q] = b->sims[q]->tm[0];
-      tm[2 * (size_t)q + 1] = b->sims[q]->tm[1];
+      lbm_sim* h = b->sims[q];
+      for (int k = 0; k < 2; ++k) {
+        CUtensorMap* fm = &tm[4 * (size_t)q + k];
+        CUtensorMap* om = &tm[4 * (size_t)q + 2 + k];
+        if ((rc = encode_f_map(h, h->f[k], fm, BATCH_TMA_TW, BATCH_TMA_TR))) return fail(rc);
+        *om = *fm;
+        if (h->om[k] && (rc = encode_om_map(h, h->om[k], om, BATCH_TMA_TW, BATCH_TMA_TR)))
+          return fail(rc);
+      }
     }
     if ((rc = dalloc(&b->d_tmaps, tm.size()))) return fail(rc);
     if (cudaMemcpy(b->d_tmaps, tm.data(), tm.size() * sizeof(CUtensorMap),

@@ -6,8 +6,9 @@ namespace lbm {
 cudaError_t launch_init_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_INIT);
 }
-cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s) {
-  return launch_step_tma<float>(a, tm, s);
+cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, const CUtensorMap* tmo,
+                             cudaStream_t s) {
+  return launch_step_tma<float>(a, tm, tmo, s);
 }
 cudaError_t launch_output_fp32(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<float>(a, s, MODE_OUTPUT);

@@ -8,8 +8,9 @@ namespace lbm {
 cudaError_t launch_init_fp64(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<double>(a, s, MODE_INIT);
 }
-cudaError_t launch_step_fp64(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s) {
-  return launch_step_tma<double>(a, tm, s);
+cudaError_t launch_step_fp64(const LatticeArgs& a, const CUtensorMap* tm, const CUtensorMap* tmo,
+                             cudaStream_t s) {
+  return launch_step_tma<double>(a, tm, tmo, s);
 }
 cudaError_t launch_output_fp64(const LatticeArgs& a, cudaStream_t s) {
   return launch_mode<double>(a, s, MODE_OUTPUT);

@@ -194,11 +194,13 @@ struct LatticeArgs {
 
 // Launchers (defined in lbm_fp64.cu / lbm_fp32.cu).
 cudaError_t launch_init_fp64(const LatticeArgs& a, cudaStream_t s);
-cudaError_t launch_step_fp64(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s);
+cudaError_t launch_step_fp64(const LatticeArgs& a, const CUtensorMap* tm, const CUtensorMap* tmo,
+                             cudaStream_t s);
 cudaError_t launch_output_fp64(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_restart_fp64(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_init_fp32(const LatticeArgs& a, cudaStream_t s);
-cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s);
+cudaError_t launch_step_fp32(const LatticeArgs& a, const CUtensorMap* tm, const CUtensorMap* tmo,
+                             cudaStream_t s);
 cudaError_t launch_output_fp32(const LatticeArgs& a, cudaStream_t s);
 cudaError_t launch_restart_fp32(const LatticeArgs& a, cudaStream_t s);
 // One time step of the BGK collision (one node per thread).
@@ -237,10 +239,11 @@ struct BatchSim {
 };
 
 // Batch tile shapes (nodes): 0: 32 x 8, 1: 64 x 4, 2: 128 x 2 (one node per
-// thread); BATCH_SHAPE_TMA: the TMA-staged tiles of the step kernel (128 x 4
-// FP32, 64 x 8 FP64), MRT models only.
+// thread); BATCH_SHAPE_TMA: the TMA-staged step kernel's pipeline on tiles of
+// 64 x 8 nodes, MRT models only.
 constexpr int BATCH_SHAPES = 3;
 constexpr int BATCH_SHAPE_TMA = 3;
+constexpr int BATCH_TMA_TW = 64, BATCH_TMA_TR = 8;  // its tile, both precisions
 __host__ __device__ constexpr int batch_bx(int shape) { return shape == 0 ? 32 : (shape == 1 ? 64 : 128); }
 __host__ __device__ constexpr int batch_by(int shape) { return 256 / batch_bx(shape); }
 
@@ -249,7 +252,8 @@ cudaError_t launch_batch_fp32(const BatchSim* sims, int nsim, long long total, i
 cudaError_t launch_batch_fp64(const BatchSim* sims, int nsim, long long total, int shape,
                               int bgk, int grid, cudaStream_t s);
 // The TMA-staged batched step: tensor maps of f[0], f[1] per simulation
-// (tmaps[2 q + b]), BatchSim::first / nbx counted in step-kernel tiles.
+// (tmaps[4 q + b]) and of om[0], om[1] (tmaps[4 q + 2 + b]), BatchSim::first /
+// nbx counted in step-kernel tiles.
 cudaError_t launch_batch_tma_fp32(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,
                                   long long total, int stress, int grid, cudaStream_t s);
 cudaError_t launch_batch_tma_fp64(const BatchSim* sims, int nsim, const CUtensorMap* tmaps,

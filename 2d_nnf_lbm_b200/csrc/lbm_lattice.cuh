@@ -455,15 +455,20 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
     } else if (gam < m.gamma_min_f) {
       nua = NU + m.m_pap_f * ty;
     } else {
-      // 1 - e^(-m gamma) by expm1f: no cancellation where m gamma is small
-      nua = NU + (ty / gam) * -expm1f(-(m.m_pap_f * gam));
+      // 1 - e^(-m gamma) by expm1f: no cancellation where m gamma is small;
+      // above m gamma = 18 it rounds to exactly 1 in FP32 (e^-18 < 2^-25),
+      // so yielded fluid skips the exponential
+      const float mg = m.m_pap_f * gam;
+      nua = NU + (ty / gam) * (mg > 18.0f ? 1.0f : -expm1f(-mg));
     }
     const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
     no.t11 = t11;
     no.t22 = t22;
     no.t12 = t12;
-    const float tm = sqrtf(0.5f * fabsf(t11 * t11 + t22 * t22 + 2.0f * (t12 * t12)));
-    no.yield = (tm <= ty) ? 5 : 0;
+    if (m.record_stress) {  // the yield flag is kept only with the stress record
+      const float tm = sqrtf(0.5f * fabsf(t11 * t11 + t22 * t22 + 2.0f * (t12 * t12)));
+      no.yield = (tm <= ty) ? 5 : 0;
+    }
     no.omega = 1.0f / (3.0f * (nua * inv_rho) + 0.5f);
   }
 }
@@ -1006,14 +1011,20 @@ __global__ void __launch_bounds__(TPB, sizeof(T) == 8 ? LBM_MINB_F64 : LBM_MINB_
 constexpr int STEP_CONSUMERS = 512;              // consumer threads (16 warps)
 constexpr int STEP_TPB = STEP_CONSUMERS + 32;    // + one producer warp
 
-template <class T>
+// TWv: nodes per tile row (the single-run kernel: 128 FP32, 64 FP64; the
+// batched kernel: 64, which leaves fewer threads idle on narrow lattices)
+template <class T, int TWv = (sizeof(T) == 8 ? 64 : 128)>
 struct Stage {
   static constexpr int H = 16 / (int)sizeof(T);               // halo: one 16-byte vector
-  static constexpr int TW = sizeof(T) == 8 ? 64 : 128;        // nodes per tile row
+  static constexpr int TW = TWv;                              // nodes per tile row
   static constexpr int TR = STEP_CONSUMERS / TW;              // tile rows (8 or 4)
   static constexpr int BW = TW + 2 * H;                       // box width (544 bytes)
   static constexpr int PLANE = TR * BW;                       // elements per plane box
-  static constexpr int BYTES = 9 * PLANE * (int)sizeof(T);
+  static constexpr int BYTES = 9 * PLANE * (int)sizeof(T);     // the population boxes
+  // a Bingham model's node omega of the tile, one box without halo after
+  // the populations (a global load per node on the collision's path otherwise)
+  static constexpr int OM_BYTES = TR * TW * (int)sizeof(T);
+  static constexpr int SLOT = BYTES + OM_BYTES;                // one stage
   // offset of population k of a node from its column in the stage
   __host__ __device__ static constexpr int off(int k) {
     return plane_of(k) * PLANE + ((k == 1 || k == 5 || k == 8) ? -1 : (k == 3 || k == 6 || k == 7) ? 1 : 0);
@@ -1044,9 +1055,9 @@ struct TileCand {
   void* om_dst;
 };
 
-template <class T>
+template <class T, class ST = Stage<T>>
 constexpr int step_smem() {
-  return NSTAGE * Stage<T>::BYTES + 2 * 8 * NSTAGE + 64 + NSTAGE * (int)sizeof(TileCand);
+  return NSTAGE * ST::SLOT + 2 * 8 * NSTAGE + 64 + NSTAGE * (int)sizeof(TileCand);
 }
 
 // Bounded wait on an mbarrier phase; false if it did not complete.
@@ -1068,10 +1079,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
 
-template <class T>
+template <class T, class ST = Stage<T>>
 __device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, uint32_t mbar,
                                          int bx, int by) {
-  using ST = Stage<T>;
   const int x = bx * ST::TW - ST::H;  // a multiple of H: 16-byte aligned
   const int y0 = by * ST::TR;
   // three boxes of three planes: row shifts c_y = 0, +1, -1 (plane_of)
@@ -1085,6 +1095,18 @@ __device__ __forceinline__ void tma_tile(const CUtensorMap* tm, uint32_t dst, ui
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y0 - cy), "r"(3 * gq), "r"(mbar)
         : "memory");
   }
+}
+
+// The node omega of tile (bx, by) of a Bingham model: one 2-D box of TR
+// rows x TW nodes, no halo (x = bx * TW is a multiple of 16 bytes).
+template <class T, class ST = Stage<T>>
+__device__ __forceinline__ void tma_omega(const CUtensorMap* tm, uint32_t dst, uint32_t mbar,
+                                          int bx, int by) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(bx * ST::TW), "r"(by * ST::TR), "r"(mbar)
+      : "memory");
 }
 
 // Candidate particles of one tile.  No latency sits between a free ring
@@ -1173,13 +1195,12 @@ struct NodeVals {
 // it gathers its populations from global memory); q points at the node's
 // stage elements.  PDL: the force accumulators are touched only after
 // griddepcontrol.wait (the particle kernel that zeroes them may still run).
-template <class T, bool PDL>
+template <class T, bool PDL, class ST = Stage<T>>
 __device__ __forceinline__ void node_gather(const LatticeArgs& a, const StepIO<T>& io,
                                             const TileCand& C, T* const q, int i, int j,
                                             bool act, bool edge, int lane, bool& waited,
                                             NodeVals<T>& v) {
   constexpr bool F64 = sizeof(T) == 8;
-  using ST = Stage<T>;
   const Geometry& g = a.g;
   const Model& m = a.m;
   const T* __restrict__ src = io.src;
@@ -1310,10 +1331,12 @@ __device__ __forceinline__ void node_gather(const LatticeArgs& a, const StepIO<T
 }
 
 // Velocity correction and collision of the next step of node (i, j) (row
-// offset nd), then its stores.
+// offset nd), then its stores.  omn: the node's omega of the previous step
+// (Bingham models; read by the caller before it releases the stage).
 template <class T, bool STRESS>
 __device__ __forceinline__ void node_collide(const LatticeArgs& a, const StepIO<T>& io,
-                                             NodeVals<T>& v, int i, int j, long long nd) {
+                                             NodeVals<T>& v, int i, int j, long long nd,
+                                             T om_node) {
   constexpr bool F64 = sizeof(T) == 8;
   const Model& m = a.m;
   const long long P = a.g.plane;
@@ -1330,7 +1353,7 @@ __device__ __forceinline__ void node_collide(const LatticeArgs& a, const StepIO<
   no.yield = 0;
   no.t11 = no.t22 = no.t12 = 0.0;
   T omn = (T)m.omega;
-  if (bingham) omn = io.om_src[nd];
+  if (bingham) omn = om_node;
   if (F64) {
     double S[9];
     if (bingham) {
@@ -1380,16 +1403,17 @@ __device__ __forceinline__ void node_collide(const LatticeArgs& a, const StepIO<
 // STRESS: the model needs the strain rate (Bingham viscosity or recorded
 // stress); the Newtonian instantiation carries none of that code.
 template <class T, bool STRESS>
-__device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMap& tm) {
+__device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMap& tm,
+                                          const CUtensorMap& tmo) {
   constexpr bool F64 = sizeof(T) == 8;
   constexpr uint32_t WAIT = 1u << 20;
   using ST = Stage<T>;
   extern __shared__ __align__(128) unsigned char s_raw[];
   T* const stage_w = reinterpret_cast<T*>(s_raw);
   const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(s_raw);
-  const uint32_t full0 = s_base + NSTAGE * ST::BYTES;  // NSTAGE "full" barriers
+  const uint32_t full0 = s_base + NSTAGE * ST::SLOT;  // NSTAGE "full" barriers
   const uint32_t empty0 = full0 + 8 * NSTAGE;          // NSTAGE "empty" barriers
-  TileCand* cands = reinterpret_cast<TileCand*>(s_raw + NSTAGE * ST::BYTES + 16 * NSTAGE + 64);
+  TileCand* cands = reinterpret_cast<TileCand*>(s_raw + NSTAGE * ST::SLOT + 16 * NSTAGE + 64);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -1505,10 +1529,12 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
         } else {
           // boxes reaching past the lattice are filled with zeros; they
           // still deliver their full byte count
+          const bool om = STRESS && m.bingham;
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
-                       "r"((uint32_t)ST::BYTES)
+                       "r"((uint32_t)(ST::BYTES + (om ? ST::OM_BYTES : 0)))
                        : "memory");
-          tma_tile<T>(&tm, s_base + sidx * ST::BYTES, fb, bx, by);
+          tma_tile<T>(&tm, s_base + sidx * ST::SLOT, fb, bx, by);
+          if (om) tma_omega<T>(&tmo, s_base + sidx * ST::SLOT + ST::BYTES, fb, bx, by);
         }
       }
       // the candidates, while the boxes are in flight; second arrival
@@ -1599,9 +1625,16 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     // this node's nine stage elements: planes in plane_of order, the row
     // shift is in the box, the column shift -c_x is applied in ST::off.  Pull
     // streaming is a bijection, so no other node reads these elements.
-    T* const q = stage_w + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
+    T* const slot = stage_w + sidx * (ST::SLOT / (int)sizeof(T));
+    T* const q = slot + tr * ST::BW + ST::H + tc;
+    // the staged omega (none in a tile whose nodes all gather: bx * TW >= NX)
+    const T* const omq = (STRESS && m.bingham && bx * ST::TW < g.nx)
+                             ? slot + ST::BYTES / (int)sizeof(T) + tid
+                             : nullptr;
     NodeVals<T> v;
     node_gather<T, true>(a, io, C, q, i, j, act, edge, lane, waited, v);
+    // the node's omega, from the stage while it is still this tile's
+    const T omn = (STRESS && m.bingham && act) ? (omq ? *omq : io.om_src[nd]) : (T)0;
     // the stage and its candidates are consumed
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
@@ -1610,7 +1643,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     if (rslot >= 0 && act)
       mass_q += F64 ? __double2ll_rn((double)v.drho * MASS_FIX)
                     : mass_share32((float)v.drho);
-    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd);
+    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd, omn);
   }
   if (rslot >= 0) {
 #pragma unroll
@@ -1623,16 +1656,21 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
 // holds 5 of them, which caps FP64 at 96 registers per thread).
 template <class T, bool STRESS>
 __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F32)
-    k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm) {
-  step_body<T, STRESS>(a, tm);
+    k_step(const LatticeArgs a, const __grid_constant__ CUtensorMap tm,
+           const __grid_constant__ CUtensorMap tmo) {
+  step_body<T, STRESS>(a, tm, tmo);
 }
 
+// tm: the population buffer read; tmo: its omega buffer (Bingham models;
+// any map otherwise, not read)
 template <class T>
-cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStream_t s) {
+cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, const CUtensorMap* tmo,
+                            cudaStream_t s) {
   using ST = Stage<T>;
   constexpr int SMEM = step_smem<T>();
   const int sx = (a.m.bingham || a.m.record_stress) ? 1 : 0;
-  void (*const kern)(const LatticeArgs, const CUtensorMap) = sx ? k_step<T, true> : k_step<T, false>;
+  void (*const kern)(const LatticeArgs, const CUtensorMap, const CUtensorMap) =
+      sx ? k_step<T, true> : k_step<T, false>;
   static int grid_of[2][64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1668,19 +1706,21 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, a, *tm);
+  return cudaLaunchKernelEx(&cfg, kern, a, *tm, *tmo);
 }
 
 // ---------------------------------------------------------------------------
 // Batched step on the TMA pipeline: the warp-specialised step of k_step over
 // the tiles of every simulation of a batch (MRT models; a batch with a BGK
-// run takes the one-node-per-thread kernel below).  Tiles are numbered
+// run takes the one-node-per-thread kernel below), in tiles of 64 x 8 nodes
+// (a batch's lattices are often narrow: 128-wide tiles left about a sixth
+// of their threads without a node on 129-513-node rows).  Tiles are numbered
 // simulation by simulation (row-major inside one, BatchSim::first), and
 // block b takes a contiguous range of them, so it stays in one or two
 // simulations.  Entering a simulation, the producer reads its device
 // counters (step number, ping-pong buffer, history slot, list buffer: a
-// captured graph replays unchanged) and picks the tensor map of that buffer
-// (two per simulation, in global memory).  Per tile it issues the boxes,
+// captured graph replays unchanged) and picks the tensor maps of that buffer
+// and of its omega (four per simulation, in global memory).  Per tile it issues the boxes,
 // stages the candidates and notes the tile's simulation, buffers and step in
 // the stage; the simulation's LatticeArgs go into a slot of a small shared
 // ring that the consumers read their model from.  A slot is rewritten only
@@ -1691,8 +1731,13 @@ cudaError_t launch_step_tma(const LatticeArgs& a, const CUtensorMap* tm, cudaStr
 constexpr int BATCH_ARGS_SLOTS = 2 * NSTAGE;
 
 template <class T>
+using BatchStage = Stage<T, BATCH_TMA_TW>;
+static_assert(BatchStage<float>::TR == BATCH_TMA_TR && BatchStage<double>::TR == BATCH_TMA_TR,
+              "batched TMA tile");
+
+template <class T>
 constexpr int batch_step_smem() {
-  return step_smem<T>() + BATCH_ARGS_SLOTS * (int)sizeof(LatticeArgs);
+  return step_smem<T, BatchStage<T>>() + BATCH_ARGS_SLOTS * (int)sizeof(LatticeArgs);
 }
 
 template <class T, bool STRESS>
@@ -1701,14 +1746,14 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F
                  const CUtensorMap* __restrict__ tmaps, long long total) {
   constexpr bool F64 = sizeof(T) == 8;
   constexpr uint32_t WAIT = 1u << 20;
-  using ST = Stage<T>;
+  using ST = BatchStage<T>;
   static_assert(sizeof(LatticeArgs) % 8 == 0 && sizeof(TileCand) % 8 == 0, "8-byte words");
   extern __shared__ __align__(128) unsigned char s_raw[];
   T* const stage_w = reinterpret_cast<T*>(s_raw);
   const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(s_raw);
-  const uint32_t full0 = s_base + NSTAGE * ST::BYTES;
+  const uint32_t full0 = s_base + NSTAGE * ST::SLOT;
   const uint32_t empty0 = full0 + 8 * NSTAGE;
-  unsigned char* const cand_raw = s_raw + NSTAGE * ST::BYTES + 16 * NSTAGE + 64;
+  unsigned char* const cand_raw = s_raw + NSTAGE * ST::SLOT + 16 * NSTAGE + 64;
   TileCand* cands = reinterpret_cast<TileCand*>(cand_raw);
   LatticeArgs* ring = reinterpret_cast<LatticeArgs*>(cand_raw + NSTAGE * sizeof(TileCand));
   __shared__ int s_ring_sim[BATCH_ARGS_SLOTS];
@@ -1747,6 +1792,7 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F
     long long first = 0, next = 0, kk = 0;
     int ntx = 1, ltx = 1, nx = 0, buf = 0, lbuf = 0, rslot = -1;
     const CUtensorMap* tm = nullptr;
+    bool om = false;
     auto enter = [&](int sq) {
       const BatchSim& B = sims[sq];
       long long k = 0, f0 = 0, f1 = 0;
@@ -1768,7 +1814,8 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F
       ntx = B.nbx;
       ltx = B.a.g.ltx;
       nx = B.a.g.nx;
-      tm = tmaps + 2 * sq + buf;
+      tm = tmaps + 4 * sq + buf;
+      om = STRESS && B.a.m.bingham;
     };
     if (t_lo < t_hi) enter(q);
     int sidx = 0, n = 0;
@@ -1822,9 +1869,10 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F
           mbar_arrive(fb);  // every node on the right edge gathers from global memory
         } else {
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb),
-                       "r"((uint32_t)ST::BYTES)
+                       "r"((uint32_t)(ST::BYTES + (om ? ST::OM_BYTES : 0)))
                        : "memory");
-          tma_tile<T>(tm, s_base + sidx * ST::BYTES, fb, bx, by);
+          tma_tile<T, ST>(tm, s_base + sidx * ST::SLOT, fb, bx, by);
+          if (om) tma_omega<T, ST>(tm + 2, s_base + sidx * ST::SLOT + ST::BYTES, fb, bx, by);
         }
       }
       cand_copy(B.a, cl, bx, by, C, lane, fb);
@@ -1895,15 +1943,21 @@ __global__ void __launch_bounds__(STEP_TPB, sizeof(T) == 8 ? 1 : LBM_STEP_MINB_F
     }
     const bool act = (i <= g.nx) && (j <= g.ny);
     const bool edge = (i == 0) || (i >= g.nx) || (j == 0) || (j >= g.ny);
-    T* const qp = stage_w + sidx * (ST::BYTES / (int)sizeof(T)) + tr * ST::BW + ST::H + tc;
+    T* const slot = stage_w + sidx * (ST::SLOT / (int)sizeof(T));
+    T* const qp = slot + tr * ST::BW + ST::H + tc;
+    const T* const omq = (STRESS && a.m.bingham && bx * ST::TW < g.nx)
+                             ? slot + ST::BYTES / (int)sizeof(T) + tid
+                             : nullptr;
     NodeVals<T> v;
-    node_gather<T, false>(a, io, C, qp, i, j, act, edge, lane, waited, v);
+    node_gather<T, false, ST>(a, io, C, qp, i, j, act, edge, lane, waited, v);
+    // the node's omega, from the stage while it is still this tile's
+    const T omn = (STRESS && a.m.bingham && act) ? (omq ? *omq : io.om_src[nd]) : (T)0;
     // the stage and its candidates are consumed (the ring slot is not)
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * sidx);
     if (cur_rslot >= 0 && cur_mass != nullptr && act)
       mass_q += F64 ? __double2ll_rn((double)v.drho * MASS_FIX) : mass_share32((float)v.drho);
-    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd);
+    if (act) node_collide<T, STRESS>(a, io, v, i, j, nd, omn);
   }
   flush_mass();
 }

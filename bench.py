@@ -33,8 +33,8 @@ Objects of the JSON line beside the headline (N=1; --parts selects them):
 --profile-run CASE runs one workload for a few steps with no timing around
 it, for ncu captures of single launches: step-fp32 / step-fp64 (the bench
 workload), adjoint (the adjoint workload, objective over the last 100 steps),
-batch (the first --batch-sims runs of the batched workload, 32x8 tiles, 6
-blocks per SM).
+batch (the first --batch-sims runs of the batched workload on the
+TMA-staged batched kernel).
 
 Multi-GPU: the hot path does not shard (one simulation, one GPU); --gpus N
 runs N independent replicas (weak scaling), timed as the max over ranks.
@@ -244,13 +244,15 @@ def run_gpu_path(pkg, torch, args, precision, device, world, dist, clocks=False)
     p.device = device
     sim = pkg.Simulation(p)
     sim.set_particles(pin)
+    # the clock sampler starts first (it takes ~0.3 s): the warm-up steps run
+    # after that idle gap, and the timed steps right after them
+    sampler = ClockSampler(device) if clocks else None
+    if sampler:
+        sampler.start()
     sim.step(args.warmup)
     sim.series()
     if dist is not None:
         dist.barrier()
-    sampler = ClockSampler(device) if clocks else None
-    if sampler:
-        sampler.start()
     ms = time_steps(pkg, torch, sim, args.steps)
     clk = sampler.stop() if sampler else None
     ms = reduce_max(dist, torch, ms, f"cuda:{device}")
@@ -844,7 +846,7 @@ def profile_run(pkg, args):
     if args.profile_run == "batch":
         cs = pkg.cases.workload_cfg4(1)[: args.batch_sims]
         b = pkg.Batch([q for q, _ in cs])
-        b.set_tuning(32, 8, 6)
+        b.set_tuning(64, 8, 2)  # the TMA-staged batched tiles
         for s, (_, disks) in zip(b.sims, cs):
             s.set_particles(disks)
         b.step(args.steps)

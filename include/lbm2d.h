@@ -324,8 +324,8 @@ int lbm_adjoint(lbm_sim* h, const lbm_objective* obj, double* value, double* gra
  * (lbm_set_particles, the getters, lbm_get_state ...); do not call
  * lbm_step on it while it belongs to a batch.  The first lbm_batch_step
  * picks the lattice kernel by timing each candidate on live steps: the
- * TMA-staged tiles of the single-run step kernel (128x4 FP32 / 64x8 FP64
- * nodes, at their own occupancy; batches without a BGK run) or the
+ * single-run step kernel's TMA pipeline on tiles of 64x8 nodes (at its own
+ * occupancy; batches without a BGK run) or the
  * one-node-per-thread kernel at a tile shape of 32x8, 64x4 or 128x2 nodes
  * and a persistent grid of 2, 4 or 6 blocks per SM; the results do not
  * depend on the choice.  lbm_batch_set_tuning fixes it instead (tile_x 0:

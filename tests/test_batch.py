@@ -176,7 +176,7 @@ def test_batch_mrt_runs_match_the_oracle(pkg, cases, precision, rtol, tma):
 
 
 def _tma_shape(precision):
-    return (64, 8, 1) if precision == 0 else (128, 4, 2)
+    return (64, 8, 2)  # the TMA-staged batched tiles, both precisions
 
 
 @pytest.mark.parametrize("precision", [0, 1])
