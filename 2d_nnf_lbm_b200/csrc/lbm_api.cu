@@ -53,7 +53,7 @@ struct lbm_sim {
   int* tile_count = nullptr;
   int* tile_list = nullptr;
   int* tile_cur = nullptr;
-  int* tile_order = nullptr;  // [2][ntiles]
+  int* tile_order = nullptr;  // [2 buffers][forward, reversed][ntiles]
   int* n_unlisted = nullptr;  // [2]
   int* work_ctr = nullptr;    // [2]
   int tile_cap = MAX_TILE_CAND;
@@ -1050,7 +1050,7 @@ int lbm_create(const lbm_params* pin, lbm_sim** out) {
   if ((rc = dalloc(&h->tile_count, (size_t)2 * ntiles))) return fail(rc);
   if ((rc = dalloc(&h->tile_list, (size_t)2 * ntiles * h->tile_cap))) return fail(rc);
   if ((rc = dalloc(&h->tile_cur, 2))) return fail(rc);
-  if ((rc = dalloc(&h->tile_order, (size_t)2 * ntiles))) return fail(rc);
+  if ((rc = dalloc(&h->tile_order, (size_t)4 * ntiles))) return fail(rc);
   if ((rc = dalloc(&h->n_unlisted, 2))) return fail(rc);
   if ((rc = dalloc(&h->work_ctr, 2))) return fail(rc);
   cudaMemsetAsync(h->work_ctr, 0, 2 * sizeof(int), h->stream);

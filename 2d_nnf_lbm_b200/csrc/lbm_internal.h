@@ -120,7 +120,8 @@ struct ParticleArgs {
   int* tile_count;           // [2][ntiles]
   int* tile_list;            // [2][ntiles][tile_cap]
   int* tile_cur;             // [2]: list buffer valid for step k at [k&1]
-  int* tile_order;           // [2][ntiles]: list tiles, those without disks first
+  int* tile_order;           // [2][2][ntiles]: list tiles, those without disks first;
+                             // forward and with each group reversed
   int* n_unlisted;           // [2]: how many list tiles have no disk
   int* work_ctr;             // [2]: step-kernel tile queue of step k at [k&1]
   int tile_cap;
@@ -169,7 +170,8 @@ struct LatticeArgs {
   const int* tile_count; // [2][ntiles]
   const int* tile_list;
   const int* tile_cur;   // [2]: list buffer valid for step k at [k&1]
-  const int* tile_order; // [2][ntiles]: list tiles, those without disks first
+  const int* tile_order; // [2][2][ntiles]: list tiles, those without disks first;
+                         // forward and with each group reversed (odd steps)
   const int* n_unlisted; // [2]
   int* work_ctr;         // [2]: tile queue of step k at [k&1], zero at the start
   int tile_cap;

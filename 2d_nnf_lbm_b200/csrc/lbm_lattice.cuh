@@ -1422,6 +1422,10 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
   const int ntx = (g.nx + 1 + ST::TW - 1) / ST::TW;
   const int nty = (g.ny + 1 + ST::TR - 1) / ST::TR;
 
+  if (tid == STEP_CONSUMERS) {  // the producer's descriptors, before its first issue
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm)) : "memory");
+    if (STRESS) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmo)) : "memory");
+  }
   if (tid == 0) {
     for (int st = 0; st < NSTAGE; ++st) {
       // "full": the TMA boxes (expect_tx) and the candidates, two arrivals
@@ -1459,8 +1463,10 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
     int t0 = (int)blockIdx.x, t1 = (int)gridDim.x + (int)blockIdx.x, t2 = 0;
     int L0 = 0, L1 = 0, L2 = 0, nu = 0, bo = 0;
     if (lane == 0) {
-      const int* o0 = a.tile_order;
-      const int* o1 = a.tile_order + a.ntiles;
+      // odd steps take each group of the order reversed (tile_order[2 buf + 1])
+      const int dir = (int)(a.step & 1);
+      const int* o0 = a.tile_order + (long long)dir * a.ntiles;
+      const int* o1 = a.tile_order + (long long)(2 + dir) * a.ntiles;
       bo = a.tile_cur[(a.step - 1) & 1];
       const int nu0 = a.n_unlisted[0], nu1 = a.n_unlisted[1];
       const int a0 = t0 < Q ? o0[t0 / S] : 0, a1 = t0 < Q ? o1[t0 / S] : 0;
@@ -1471,7 +1477,7 @@ __device__ __forceinline__ void step_body(const LatticeArgs& a, const CUtensorMa
       L1 = bo ? b1 : b0;
     }
     const int buf_old = __shfl_sync(0xffffffffu, bo, 0);
-    const int* order = a.tile_order + (long long)buf_old * a.ntiles;
+    const int* order = a.tile_order + (long long)(2 * buf_old + (int)(a.step & 1)) * a.ntiles;
     int buf = -1;
     bool waited = false;
     int sidx = 0;

@@ -97,14 +97,18 @@ __device__ __forceinline__ void insert_tiles(const ParticleArgs& a, int p, doubl
 }
 
 // Order of the list tiles of buffer buf for the step kernel's tile queue:
-// the tiles without disks first, then those with, each group in index order;
-// n_unlisted[buf] = size of the first group.  Run by one block.
+// the tiles without disks first, then those with, each group in index order
+// (tile_order[2 buf]) and each group reversed (tile_order[2 buf + 1], for odd
+// steps: a step then starts on the rows the previous one wrote last, which
+// are still in L2); n_unlisted[buf] = size of the first group.  Run by one
+// block.
 __device__ void build_tile_order(const ParticleArgs& a, int buf) {
   __shared__ int s_w[PBLK / 32];
   __shared__ int s_base[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x / 32;
   const int* cnt = a.tile_count + (long long)buf * a.ntiles;
-  int* ord = a.tile_order + (long long)buf * a.ntiles;
+  int* ord = a.tile_order + (long long)(2 * buf) * a.ntiles;
+  int* rev = ord + a.ntiles;
   int nu = 0;
   for (int t = tid; t < a.ntiles; t += blockDim.x) nu += cnt[t] == 0 ? 1 : 0;
   for (int o = 16; o > 0; o >>= 1) nu += __shfl_xor_sync(0xffffffffu, nu, o);
@@ -133,8 +137,15 @@ __device__ void build_tile_order(const ParticleArgs& a, int buf) {
       chunk += s_w[w];
     }
     const int ex = before + inc - v;
-    if (un) ord[s_base[0] + (ex & 0xffff)] = t;
-    else if (in) ord[total_u + s_base[1] + (ex >> 16)] = t;
+    if (un) {
+      const int pos = s_base[0] + (ex & 0xffff);
+      ord[pos] = t;
+      rev[total_u - 1 - pos] = t;
+    } else if (in) {
+      const int pos = total_u + s_base[1] + (ex >> 16);
+      ord[pos] = t;
+      rev[a.ntiles - 1 + total_u - pos] = t;
+    }
     __syncthreads();
     if (tid == 0) {
       s_base[0] += chunk & 0xffff;
