@@ -32,7 +32,8 @@ Objects of the JSON line beside the headline (N=1; --parts selects them):
 
 --profile-run CASE runs one workload for a few steps with no timing around
 it, for ncu captures of single launches: step-fp32 / step-fp64 (the bench
-workload), adjoint (the adjoint workload, objective over the last 100 steps),
+workload), visco (the viscoplastic workload at Bn = 2, FP32), adjoint (the
+adjoint workload, objective over the last 100 steps),
 batch (the first --batch-sims runs of the batched workload on the
 TMA-staged batched kernel).
 
@@ -63,8 +64,9 @@ BINGHAM_BYTES_PER_NODE = {0: 160.0, 1: 80.0}  # + per-node omega read and writte
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one k_step<float> launch of the bench workload,
 # from ncu (dram__bytes_read.sum + dram__bytes_write.sum, one launch, cold);
-# the capture and its command are in profiles/k_step_fp32_sedimentation_1024x2048.md
-K_STEP_FP32_TRAFFIC = {"bytes": 111724800.0, "captured_at": "11ba40b"}
+# captured with `ncu --set full -k regex:k_step -s 5 -c 1` on
+# `python bench.py --profile-run step-fp32 --steps 30` (summary under profiles/)
+K_STEP_FP32_TRAFFIC = {"bytes": 112485888.0, "captured_at": "0e24264"}
 PARTS = ("fp32", "fp64", "e2e", "trajectory", "viscoplastic", "adjoint", "batch", "cpu")
 
 
@@ -94,7 +96,7 @@ def parse_args(argv=None):
     ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--particles", type=int, default=512)
     ap.add_argument("--profile-run", default="",
-                    choices=["", "step-fp32", "step-fp64", "adjoint", "batch"])
+                    choices=["", "step-fp32", "step-fp64", "visco", "adjoint", "batch"])
     a = ap.parse_args(argv)
     parts = set(PARTS) if a.parts == "all" else {s.strip() for s in a.parts.split(",") if s.strip()}
     unknown = parts - set(PARTS)
@@ -336,15 +338,24 @@ def trajectory_error(pkg, args, device, steps):
     timed region, at milestones up to `steps` steps (the multi-particle
     configuration runs 50,000): the largest disk displacement error
     relative to the largest FP64 displacement, and the same for the velocity
-    (the FP64 path matches the oracle within 1e-10 on the parity cases)."""
+    (the FP64 path matches the oracle within 1e-10 on the parity cases).
+    Control: a second FP64 run whose only change is the disks' initial
+    centres rounded to FP32 (what a single-precision input file would hold);
+    its departure from the first FP64 run is the suspension's own
+    sensitivity to a perturbation of that size."""
     sims = {}
     pin = None
-    for prec in (1, 0):
-        p, pin = workload(pkg, prec, args)
+    for prec in (1, 0, "ctl"):
+        p, pin = workload(pkg, 0 if prec == "ctl" else prec, args)
         p.device = device
         p.series_every = 0
         sims[prec] = pkg.Simulation(p)
-        sims[prec].set_particles(pin)
+        if prec == "ctl":
+            q = pin.copy()
+            q[:, 0:2] = q[:, 0:2].astype(np.float32).astype(np.float64)
+            sims[prec].set_particles(q)
+        else:
+            sims[prec].set_particles(pin)
     marks = sorted({m for m in (2000, 10000, 20000, 30000, 40000, steps) if m <= steps})
     tiny = 1e-300
     at = []
@@ -360,6 +371,8 @@ def trajectory_error(pkg, args, device, steps):
         vmax = max(float(np.max(np.linalg.norm(v64, axis=1))), tiny)
         ed = np.linalg.norm(d32 - d64, axis=1) / dmax
         ev = np.linalg.norm(v32 - v64, axis=1) / vmax
+        rc = sims["ctl"].particles()
+        ec = np.linalg.norm(rc[:, 0:2] - r64[:, 0:2], axis=1) / dmax
         at.append({
             "steps": m,
             "max_rel_displacement_err": float(ed.max()),
@@ -367,7 +380,9 @@ def trajectory_error(pkg, args, device, steps):
             "max_rel_velocity_err": float(ev.max()),
             "rms_rel_velocity_err": float(np.sqrt(np.mean(ev ** 2))),
             "max_fp64_displacement": float(np.max(np.linalg.norm(d64, axis=1))),
-            "status": [sims[1].status(), sims[0].status()],
+            "control_max_rel_displacement_err": float(ec.max()),
+            "control_rms_rel_displacement_err": float(np.sqrt(np.mean(ec ** 2))),
+            "status": [sims[1].status(), sims[0].status(), sims["ctl"].status()],
         })
     for s in sims.values():
         s.close()
@@ -381,6 +396,10 @@ def trajectory_error(pkg, args, device, steps):
         "tolerance": 1e-4,
         "within_tolerance": bool(last["max_rel_displacement_err"] <= 1e-4 and
                                  last["max_rel_velocity_err"] <= 1e-4),
+        "rms_within_tolerance": bool(last["rms_rel_displacement_err"] <= 1e-4),
+        "control": "FP64 with the initial centres rounded to FP32, against FP64",
+        "control_max_rel_displacement_err": last["control_max_rel_displacement_err"],
+        "control_rms_rel_displacement_err": last["control_rms_rel_displacement_err"],
         "milestones": at,
     }
 
@@ -854,6 +873,15 @@ def profile_run(pkg, args):
         print(f"steps {b.sims[0].kk}  run 0 disk at ({parts[0, 0]:.6f}, {parts[0, 1]:.6f})  "
               f"status {max(abs(s.status()) for s in b.sims)}")
         b.close()
+        return 0
+    if args.profile_run == "visco":
+        p, pin, _ = pkg.cases.workload_cfg3(1, 2.0)
+        with pkg.Simulation(p) as sim:
+            sim.set_particles(pin)
+            sim.step(args.steps)
+            parts = sim.particles()
+            print(f"steps {sim.kk}  disk at ({parts[0, 0]:.6f}, {parts[0, 1]:.6f})  "
+                  f"status {sim.status()}")
         return 0
     prec = 1 if args.profile_run == "step-fp32" else 0
     p, pin = workload(pkg, prec, args)
