@@ -61,6 +61,8 @@ struct lbm_sim {
   int* nbr_count = nullptr;
   double* nbr_xy = nullptr;
   int* pair_rebuild = nullptr;
+  double* ps_pin = nullptr;     // pinned staging of the particle upload [PS][npad]
+  size_t ps_pin_n = 0;          // its size in doubles
   bool partials_valid = false;  // facc holds FORCE of the last lattice step
   int ncx = 1, ncy = 1;
   double cell_size = 1.0;
@@ -552,49 +554,60 @@ int read_particles(lbm_sim* h, std::vector<double>& buf) {
   return LBM_OK;
 }
 
-// Upload np AoS records (PS doubles each) into the SoA device layout.
+// Upload np AoS records (PS doubles each) into the SoA device layout,
+// through the handle's pinned staging buffer (a direct DMA copy).  Both
+// callers (lbm_set_particles, lbm_set_state) synchronise the stream before
+// the call and after it, so no copy from the buffer is in flight when it is
+// refilled.
 int write_particles(lbm_sim* h, const std::vector<double>& buf) {
   const size_t npad = (size_t)h->npad;
-  std::vector<double> soa(npad * PS, 0.0);
+  const size_t n = npad * PS;
+  if (h->ps_pin_n < n) {
+    if (h->ps_pin) cudaFreeHost(h->ps_pin);
+    h->ps_pin = nullptr;
+    h->ps_pin_n = 0;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&h->ps_pin), n * sizeof(double),
+                      cudaHostAllocDefault) != cudaSuccess)
+      return LBM_E_NOMEM;
+    h->ps_pin_n = n;
+  }
+  double* soa = h->ps_pin;
+  std::fill(soa, soa + n, 0.0);
   for (int i = 0; i < h->np; ++i)
     for (int f = 0; f < PS; ++f) soa[(size_t)f * npad + i] = buf[(size_t)i * PS + f];
-  // from pageable memory: the call returns once soa has been staged, so the
-  // vector may go out of scope without a stream synchronisation
-  CK(h2d(h, h->ps, soa.data(), soa.size() * sizeof(double)));
+  CK(h2d(h, h->ps, soa, n * sizeof(double)));
   return LBM_OK;
 }
 
 // Whether two input disks overlap (centre distance below the sum of the
-// radii), by a cell grid of the largest diameter: O(np) on the host.
-bool disks_overlap(const double* pin, int np, double dmax) {
+// radii), on the host in O(np + cells): a linked-cell grid over the lattice
+// whose cells are at least the largest diameter wide (so two overlapping
+// disks lie in the same or in adjacent cells) and few enough (about np) that
+// clearing it costs no more than the disks.  Centres lie in [0, nx] x [0, ny]
+// (checked by the caller).
+bool disks_overlap(const double* pin, int np, double dmax, int nx, int ny) {
   if (np < 2 || !(dmax > 0.0)) return false;
-  const double cs = dmax;
-  std::vector<std::pair<long long, int>> key((size_t)np);
+  const double cs = std::max(dmax, std::sqrt((nx + 1.0) * (ny + 1.0) / np));
+  const int ncx = (int)std::floor(nx / cs) + 1, ncy = (int)std::floor(ny / cs) + 1;
+  std::vector<int> head((size_t)ncx * ncy, -1), next((size_t)np), cell((size_t)np);
   for (int i = 0; i < np; ++i) {
     const double* r = pin + (size_t)LBM_PIN * i;
-    const long long cx = (long long)std::floor(r[0] / cs), cy = (long long)std::floor(r[1] / cs);
-    key[(size_t)i] = {cy * 1000003LL + cx, i};
+    const int cx = std::min(ncx - 1, (int)(r[0] / cs)), cy = std::min(ncy - 1, (int)(r[1] / cs));
+    cell[(size_t)i] = cy * ncx + cx;
+    next[(size_t)i] = head[(size_t)cell[(size_t)i]];
+    head[(size_t)cell[(size_t)i]] = i;
   }
-  std::sort(key.begin(), key.end());
-  auto cell_range = [&](long long k) {
-    auto lo = std::lower_bound(key.begin(), key.end(), std::make_pair(k, -1));
-    auto hi = std::lower_bound(key.begin(), key.end(), std::make_pair(k + 1, -1));
-    return std::make_pair(lo, hi);
-  };
   for (int i = 0; i < np; ++i) {
     const double* a = pin + (size_t)LBM_PIN * i;
-    const long long cx = (long long)std::floor(a[0] / cs), cy = (long long)std::floor(a[1] / cs);
-    for (long long dy = -1; dy <= 1; ++dy)
-      for (long long dx = -1; dx <= 1; ++dx) {
-        const auto rg = cell_range((cy + dy) * 1000003LL + cx + dx);
-        for (auto it = rg.first; it != rg.second; ++it) {
-          const int j = it->second;
+    const int cx = cell[(size_t)i] % ncx, cy = cell[(size_t)i] / ncx;
+    for (int y = std::max(0, cy - 1); y <= std::min(ncy - 1, cy + 1); ++y)
+      for (int x = std::max(0, cx - 1); x <= std::min(ncx - 1, cx + 1); ++x)
+        for (int j = head[(size_t)y * ncx + x]; j >= 0; j = next[(size_t)j]) {
           if (j <= i) continue;
           const double* b = pin + (size_t)LBM_PIN * j;
           const double ex = a[0] - b[0], ey = a[1] - b[1], rs = 0.5 * (a[6] + b[6]);
           if (ex * ex + ey * ey < rs * rs) return true;
         }
-      }
   }
   return false;
 }
@@ -742,6 +755,7 @@ void destroy_buffers(lbm_sim* h) {
   dfree(h->u0); dfree(h->err_part);
   if (h->series_pin) cudaFreeHost(h->series_pin);
   if (h->mass_pin) cudaFreeHost(h->mass_pin);
+  if (h->ps_pin) cudaFreeHost(h->ps_pin);
   for (const auto& b : h->series_pending) cudaEventDestroy(b.ev);
   for (cudaEvent_t e : h->series_ev_free) cudaEventDestroy(e);
   dfree(h->adj_slots); dfree(h->adj_ck); dfree(h->adj_ckp); dfree(h->adj_hist);
@@ -1111,7 +1125,7 @@ int lbm_set_particles(lbm_sim* h, int32_t np, const double* pin) {
   }
   // overlapping input disks (no reference input holds any; the repulsion
   // model's contact branch is for disks that come into contact while moving)
-  if (disks_overlap(pin, np, dmax)) return LBM_E_PARTICLE;
+  if (disks_overlap(pin, np, dmax, h->p.nx, h->p.ny)) return LBM_E_PARTICLE;
   // kernels still in flight may read the particle buffers reused below
   CK(cudaStreamSynchronize(h->stream));
   int rc = setup_particle_buffers(h, np, dmax);

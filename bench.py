@@ -285,12 +285,15 @@ def run_e2e(pkg, torch, args, device):
     density, what the reference writes every step (C1:264, C1:318) -- copied
     to host memory: the library keeps the records in a device ring and
     lbm_get_series drains them every E2E_CHUNK steps, each chunk's records
-    read while the next chunk runs."""
+    read while the next chunk runs.  The device ring holds two chunks, so the
+    chunk that runs writes other slots than the one whose records are
+    crossing to the host (a one-chunk ring makes every chunk's first step
+    wait for the previous chunk's copy)."""
     p, pin = workload(pkg, 1, args)
     p.device = device
     p.series_every = 1
     p.series_particles = pin.shape[0]
-    p.series_capacity = E2E_CHUNK
+    p.series_capacity = 2 * E2E_CHUNK
     sim = pkg.Simulation(p)
     pin_h = torch.from_numpy(pin).pin_memory().numpy()
     sim.set_particles(pin_h)
@@ -326,7 +329,8 @@ def run_e2e(pkg, torch, args, device):
         "value": nodes * k / (ms * 1e-3) / 1e6,
         "unit": "MLUPS",
         "h2d_bytes_per_step": pin.nbytes / k,
-        "d2h_bytes_per_step": int(rec_len * 8),
+        # the record and its fixed-point mean-density sum
+        "d2h_bytes_per_step": int(rec_len * 8 + 8),
         "wall_s": wall,
         "output": f"every step's history record ({rec_len} doubles), drained every "
                   f"{E2E_CHUNK} steps",

@@ -161,3 +161,44 @@ def test_overlapping_input_disks_are_rejected(pkg, cases):
     sim.set_particles(cases.pin_array([[20.0, 20.0], [28.0, 20.0]], 8.0, 1.25))
     assert sim.status() == 0
     sim.close()
+
+
+def _overlaps(xy, d):
+    """All pairs: some two disks closer than the sum of their radii."""
+    e = xy[:, None, :] - xy[None, :, :]
+    r2 = np.einsum("ijk,ijk->ij", e, e)
+    rs = 0.5 * (d[:, None] + d[None, :])
+    np.fill_diagonal(r2, np.inf)
+    return bool(np.any(r2 < rs * rs))
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_overlap_check_matches_all_pairs(pkg, cases, seed):
+    """The library's overlap check (a cell grid) against all pairs, on random
+    disk sets of mixed diameters: sets built without overlap are accepted,
+    the same sets with one disk moved onto another (anywhere, so across cell
+    edges too) are rejected."""
+    rng = np.random.default_rng(seed)
+    nx, ny = 300, 500
+    xy, d = [], []
+    while len(xy) < 150:
+        c = rng.uniform([0.0, 0.0], [nx, ny])
+        dd = rng.uniform(2.0, 14.0)
+        if all(np.hypot(*(c - q)) >= 0.5 * (dd + e) for q, e in zip(xy, d)):
+            xy.append(c)
+            d.append(dd)
+    xy, d = np.array(xy), np.array(d)
+    assert not _overlaps(xy, d)
+    p = cases.shipped_c1(nx, ny, 8.0)
+    sim = pkg.Simulation(p)
+    sim.set_particles(cases.pin_array(xy, d, 1.25))
+    a, b = rng.choice(len(xy), 2, replace=False)
+    xy2 = xy.copy()
+    ang = rng.uniform(0.0, 2 * np.pi)
+    xy2[a] = np.clip(xy[b] + 0.45 * (d[a] + d[b]) * np.array([np.cos(ang), np.sin(ang)]),
+                     [0.0, 0.0], [nx, ny])
+    assert _overlaps(xy2, d)
+    with pytest.raises(pkg.LbmError) as err:
+        sim.set_particles(cases.pin_array(xy2, d, 1.25))
+    assert err.value.code == LBM_E_PARTICLE
+    sim.close()
