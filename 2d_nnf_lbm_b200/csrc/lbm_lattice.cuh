@@ -436,13 +436,18 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
   no.yield = 0;
   no.omega = r.sw;
   if (m.bingham) {
-    const float inv_rho = 1.0f / rho;
+    // The divisions and the square root of the strain rate use the hardware
+    // approximations (relative errors of a few 2^-23, far below the FP32
+    // populations' own rounding after the collision); 1 - e^(-m gamma) keeps
+    // expm1f, whose accuracy at small m gamma the plug regions need.
+    const float inv_rho = __fdividef(1.0f, rho);
     if (!m.strain_feq) {
       D11 *= inv_rho;
       D22 *= inv_rho;
       D12 *= inv_rho;
     }
-    const float gam = sqrtf(2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12)));
+    const float g2 = 2.0f * fabsf(D11 * D11 + D22 * D22 + 2.0f * (D12 * D12));
+    const float gam = g2 > 0.0f ? g2 * rsqrtf(g2) : 0.0f;
     const float ty = m.tau_y_f;
     float nua;
     if (m.casson) {
@@ -459,7 +464,7 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
       // above m gamma = 18 it rounds to exactly 1 in FP32 (e^-18 < 2^-25),
       // so yielded fluid skips the exponential
       const float mg = m.m_pap_f * gam;
-      nua = NU + (ty / gam) * (mg > 18.0f ? 1.0f : -expm1f(-mg));
+      nua = NU + __fdividef(ty, gam) * (mg > 18.0f ? 1.0f : -expm1f(-mg));
     }
     const float t11 = nua * 2.0f * D11, t22 = nua * 2.0f * D22, t12 = nua * 2.0f * D12;
     no.t11 = t11;
@@ -469,7 +474,7 @@ __device__ __forceinline__ void relax32(const Model& m, const Mom32& q, float rh
       const float tm = sqrtf(0.5f * fabsf(t11 * t11 + t22 * t22 + 2.0f * (t12 * t12)));
       no.yield = (tm <= ty) ? 5 : 0;
     }
-    no.omega = 1.0f / (3.0f * (nua * inv_rho) + 0.5f);
+    no.omega = __fdividef(1.0f, 3.0f * (nua * inv_rho) + 0.5f);
   }
 }
 
