@@ -17,6 +17,7 @@
 // Built with --fmad=false: the FP64 arithmetic is operation-for-operation the
 // reference's, so the particle update is bit-identical for identical inputs.
 #include <cuda_runtime.h>
+#include <cstddef>
 
 #include "lbm_internal.h"
 
@@ -33,6 +34,16 @@ struct PShared {
   double x[MAX_PARTICLES], y[MAX_PARTICLES], d[MAX_PARTICLES];
   int scan[PBLK / 32];
 };
+// History steps: the records of the first REC_STAGE disks (12 doubles each)
+// are staged in the pair hash's part of the shared memory (cnt .. key, dead
+// after the pair lists are built) and written out coalesced.  Written one
+// disk per thread, 12 doubles at a 96-byte stride, every store of a warp
+// touches 32 sectors, and all of them go through the one SM this kernel
+// runs on.
+constexpr int REC_STAGE =
+    (int)((2 * (HASH + 1) + 2 * MAX_PARTICLES) * sizeof(int) / (12 * sizeof(double)));
+static_assert(offsetof(PShared, x) >= (size_t)REC_STAGE * 12 * sizeof(double),
+              "record staging fits in front of the centre arrays");
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -330,6 +341,8 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
   }
 
   // ---- 2. repulsion, Newton-Euler update, history -------------------------
+  double* const rstage = reinterpret_cast<double*>(smem_raw);
+  if (rec) __syncthreads();  // the pair search has finished with the hash
   for (int p = tid; p < a.np; p += PBLK) {
     const PRef P{a.ps + p, a.npad};
     // issue every global load of this disk before the dependent arithmetic
@@ -440,7 +453,7 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
     else if (nx_ < 0.0 || nx_ > (double)a.nx || ny_ < 0.0 || ny_ > (double)a.ny)
       atomicOr(a.status, ST_PARTICLE);
     if (rec && p < a.series_np) {
-      double* r = a.series + rslot * a.series_len + 2 + 12LL * p;
+      double* r = p < REC_STAGE ? rstage + 12LL * p : a.series + rslot * a.series_len + 2 + 12LL * p;
       r[0] = nx_; r[1] = ny_; r[2] = nang;
       r[3] = v0; r[4] = v1; r[5] = v2;
       r[6] = frx; r[7] = fry; r[8] = frt;
@@ -454,6 +467,11 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
     if (!(tdx * tdx + tdy * tdy <= 0.25 * SKIN * SKIN)) s_tiles = 1;
   }
   __syncthreads();
+  if (rec) {  // the staged records, coalesced
+    const int n = 12 * (a.series_np < REC_STAGE ? a.series_np : REC_STAGE);
+    double* const dst = a.series + rslot * a.series_len + 2;
+    for (int e = tid; e < n; e += PBLK) dst[e] = rstage[e];
+  }
 
   // ---- 3. tile candidate lists ---------------------------------------------
   // The lattice kernel of this step, already running, sorts its tiles by the
