@@ -41,3 +41,32 @@ def test_small_ring_matches_large_ring_bit_for_bit(pkg, cases, precision):
     assert np.array_equal(one_call, want)
     assert np.array_equal(uneven, want)
     assert np.all(np.isfinite(want))
+
+
+def test_records_of_many_disks_match_the_particle_state(pkg, cases):
+    """700 disks, each recorded every step: the particle kernel stages the
+    records of the first disks in shared memory and writes the rest
+    directly; every disk's record of the last step (centre, angle,
+    velocities, F_H_IN) equals the particle state read back after it, bit
+    for bit (both are the same values of the same kernel)."""
+    n = 700
+    xy = np.array([[12.0 + 13.0 * (k % 28), 12.0 + 14.0 * (k // 28)] for k in range(n)])
+    p = cases.shipped_c1(400, 400, 4.0)
+    p.precision = 1
+    p.series_every = 1
+    p.series_particles = n
+    p.series_capacity = 8
+    sim = pkg.Simulation(p)
+    sim.set_particles(cases.pin_array(xy, 4.0, 1.25))
+    sim.step(3)
+    s = sim.series()
+    parts = sim.particles()
+    st = sim.status()
+    sim.close()
+    assert st == 0
+    assert s.shape == (3, 2 + 12 * n)
+    assert np.array_equal(s[:, 0], [1.0, 2.0, 3.0])
+    rec = s[-1, 2:].reshape(n, 12)
+    assert np.array_equal(rec[:, 0:6], parts[:, 0:6])
+    assert np.array_equal(rec[:, 9:12], parts[:, 11:14])
+    assert np.any(rec[:, 4] != 0.0)  # the disks have started to move
