@@ -147,9 +147,19 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
         except OSError:
             self.proc = None
+            return
+        # the GPU work starts once nvidia-smi is sampling (two lines written):
+        # its start-up (driver and NVML initialisation, slower on a host
+        # with many GPUs) then lies before the warm-up, not inside a short
+        # timed region
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            with open(self.path) as fh:
+                if sum(1 for _ in fh) >= 2:
+                    break
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
