@@ -47,8 +47,8 @@ def test_selftest_limit_is_validated(pkg, cases):
 
 # ---- failures made on the host: bad states and bad inputs --------------------
 # None of these faults the GPU: each is an input that the library's own checks
-# turn into a status code (SURVEY plan: NaN detection, capacity overflows,
-# particles leaving the lattice, overlapping input disks).
+# turn into a status code: NaN detection, capacity overflows, particles
+# leaving the lattice, overlapping input disks.
 
 LBM_E_NAN, LBM_E_OVERFLOW, LBM_E_PARTICLE = -5, -7, -9
 
