@@ -4,13 +4,15 @@ tests/golden/make_adjoint_fd.py) and of the GPU's FP64 forward, FP32 against
 FP64.
 
 Tolerances: an adjoint entry g matches a difference quotient d(delta) when
-|g - d(delta/2)| <= rtol |d(delta/2)| + 4 |d(delta) - d(delta/2)| + floor.
-The second term bounds the quotient's own error; it matters for the initial
-position, where the solid-fraction profile has a kink in its second
-derivative.  floor is zero except for the initial position, whose entries
-can vanish by symmetry: there it is rtol |J| / D, rtol of the change in J
-that moving the disk by one diameter D would bring.  rtol = 1e-6 for the
-FP64 adjoint, 1e-3 for the FP32 one.  The objective itself: FP64 within
+|g - d(delta/2)| <= rtol |d(delta/2)| + |d(delta) - d(delta/2)| + floor.
+The second term is the quotient's own error: for a central difference the
+error of d(delta/2) is about a third of |d(delta) - d(delta/2)|, and it
+matters for the initial position, where the solid-fraction profile has a
+kink in its second derivative (the measured adjoint errors there are 0.3
+to 0.7 of that term).  floor is zero except for the initial position,
+whose entries can vanish by symmetry: there it is rtol times the largest
+position gradient of the case.  rtol = 1e-6 for the FP64 adjoint, 1e-3 for
+the FP32 one.  The objective itself: FP64 within
 1e-9 of the oracle's, FP32 within 1e-3.
 
 The torch.autograd.Function below exists only as a test harness: it lets
@@ -42,10 +44,12 @@ def grad_vector(g, npd):
     return np.array(out)
 
 
-def check_against_fd(grad, fd, fd_half, rtol, names, j, diam):
+def check_against_fd(grad, fd, fd_half, rtol, names):
+    pos = [k for k, nm in enumerate(names) if nm.startswith(("x0", "y0"))]
+    scale = max((abs(fd_half[k]) for k in pos), default=0.0)
     for k, nm in enumerate(names):
-        floor = rtol * abs(j) / diam if nm.startswith(("x0", "y0")) else 0.0
-        allow = rtol * abs(fd_half[k]) + 4.0 * abs(fd[k] - fd_half[k]) + floor
+        floor = rtol * scale if k in pos else 0.0
+        allow = rtol * abs(fd_half[k]) + abs(fd[k] - fd_half[k]) + floor
         assert abs(grad[k] - fd_half[k]) <= allow, (nm, grad[k], fd_half[k], allow)
 
 
@@ -94,8 +98,7 @@ def test_adjoint_matches_oracle_differences(pkg, cases, name, precision, rtol, j
     z = fixture(name)
     j, g, _ = adjoint_run(pkg, p, pin, n0, n1, precision)
     assert abs(j - float(z["j"])) <= jtol * abs(float(z["j"]))
-    check_against_fd(g, z["fd"], z["fd_half"], rtol, list(map(str, z["names"])), float(z["j"]),
-                     float(pin[0, 6]))
+    check_against_fd(g, z["fd"], z["fd_half"], rtol, list(map(str, z["names"])))
 
 
 @pytest.mark.gpu
@@ -176,8 +179,8 @@ def test_autograd_harness_fp32_against_fp64_adjoint_and_differences(pkg, cases):
     j64, g64 = _autograd_harness(pkg, p, pin, n0, n1, 0)
     j32, g32 = _autograd_harness(pkg, p, pin, n0, n1, 1)
     names = list(map(str, z["names"]))
-    check_against_fd(g64, z["fd"], z["fd_half"], 1e-6, names, float(z["j"]), float(pin[0, 6]))
-    check_against_fd(g32, z["fd"], z["fd_half"], 1e-3, names, float(z["j"]), float(pin[0, 6]))
+    check_against_fd(g64, z["fd"], z["fd_half"], 1e-6, names)
+    check_against_fd(g32, z["fd"], z["fd_half"], 1e-3, names)
     big = [0, 1, 2]  # tau_y, nu, rho_p: FP32 against the FP64 adjoint
     assert np.all(np.abs(g32[big] - g64[big]) <= 1e-3 * np.abs(g64[big]))
     assert abs(j32 - j64) <= 1e-3 * abs(j64)
@@ -217,8 +220,7 @@ def test_full_size_adjoint_against_gpu_fp64_differences(pkg, cases):
             jm = run_j(*ac.perturbed(p64, pin, name, disk, -d))
             fds.append((jp - jm) / (2 * d))
         fd, fdh = fds
-        floor = abs(j64) / float(pin[0, 6]) if name == "y0" else 0.0
         for g, rtol in ((g64[k], 1e-6), (g32[k], 1e-3)):
-            allow = rtol * abs(fdh) + 4.0 * abs(fd - fdh) + rtol * floor
+            allow = rtol * abs(fdh) + abs(fd - fdh)
             assert abs(g - fdh) <= allow, (name, g, fdh, allow)
     assert abs(j32 - j64) <= 1e-3 * abs(j64)
