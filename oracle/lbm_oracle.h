@@ -64,6 +64,19 @@ int  oracle_compute_error(oracle* o, double* er);
 /* the reference's full particle state incl. VP_OLD (np*LBM_STATE_PER) */
 int  oracle_get_state_particles(oracle* o, double* out);
 
+/* Tangent build only (liblbm_oracle_tangent.so: the same source compiled as
+ * C++ with -DORACLE_TANGENT, every real a value and its derivative): a run
+ * that carries the derivative with respect to one input, which = one of
+ * ORACLE_SEED_* (disk: the disk of rho_p, x0, y0).  Every other entry point
+ * behaves as in the ordinary build and returns the same values;
+ * oracle_get_particles_tangent returns the derivatives of what
+ * oracle_get_particles returns. */
+enum { ORACLE_SEED_TAU_Y = 0, ORACLE_SEED_NU = 1, ORACLE_SEED_RHO_P = 2, ORACLE_SEED_X0 = 3,
+       ORACLE_SEED_Y0 = 4 };
+int  oracle_create_tangent(const lbm_params* p, const oracle_opts* o, int32_t which,
+                           int32_t disk, oracle** out);
+int  oracle_get_particles_tangent(oracle* o, double* out); /* np*LBM_POUT */
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,44 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+# the inputs a tangent run can carry the derivative of (lbm_oracle.h)
+SEEDS = {"tau_y": 0, "nu": 1, "rho_p": 2, "x0": 3, "y0": 4}
+_TLIB = None
+
+
+def tangent_lib_path() -> str:
+    return os.path.join(_HERE, "liblbm_oracle_tangent.so")
+
+
+def load_tangent():
+    """The tangent build: the oracle's source compiled with every real a
+    value and its derivative (oracle_dual.h)."""
+    global _TLIB
+    if _TLIB is None:
+        if not os.path.exists(tangent_lib_path()):
+            build()
+        lib = ctypes.CDLL(tangent_lib_path())
+        P = ctypes.POINTER
+        vp = ctypes.c_void_p
+        dp = P(ctypes.c_double)
+        sigs = {
+            "oracle_create_tangent": ([P(LbmParams), P(OracleOpts), ctypes.c_int32, ctypes.c_int32,
+                                       P(vp)], ctypes.c_int),
+            "oracle_destroy": ([vp], None),
+            "oracle_set_particles": ([vp, ctypes.c_int32, dp], ctypes.c_int),
+            "oracle_step": ([vp, ctypes.c_int32], ctypes.c_int),
+            "oracle_kk": ([vp], ctypes.c_int64),
+            "oracle_get_particles": ([vp, dp], ctypes.c_int),
+            "oracle_get_particles_tangent": ([vp, dp], ctypes.c_int),
+        }
+        for name, (args, res) in sigs.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _TLIB = lib
+    return _TLIB
+
+
 class Oracle:
     """Same call sequence as ``Simulation`` but on the CPU restatement."""
 
@@ -174,3 +212,26 @@ class Oracle:
         if rc != 0:
             raise _lbm.LbmError(rc, "oracle_compute_error")
         return er.value
+
+
+class TangentOracle(Oracle):
+    """The oracle run in forward-mode derivative numbers: the same values as
+    ``Oracle`` and, beside them, their derivatives with respect to one input
+    (``which`` in SEEDS; ``disk`` for rho_p, x0, y0)."""
+
+    def __init__(self, params, which: str, disk: int = -1, omega_chain: int = 0):
+        self.lib = load_tangent()
+        self.params = params.copy()
+        self.opts = OracleOpts(omega_chain, 0, float("inf"))
+        self._h = ctypes.c_void_p()
+        rc = self.lib.oracle_create_tangent(ctypes.byref(self.params), ctypes.byref(self.opts),
+                                            SEEDS[which], int(disk), ctypes.byref(self._h))
+        if rc != 0:
+            raise _lbm.LbmError(rc, "oracle_create_tangent")
+        self.n1x, self.n1y = params.nx + 1, params.ny + 1
+        self.np = 0
+
+    def particles_tangent(self):
+        out = np.zeros((max(self.np, 1), _lbm.LBM_POUT))
+        self.lib.oracle_get_particles_tangent(self._h, _dp(out))
+        return out[: self.np]
