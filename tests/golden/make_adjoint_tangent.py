@@ -11,12 +11,19 @@ adjoint that shares no code with the CUDA adjoint kernels and has no
 finite-difference truncation error.  The omega rule is the GPU's
 (omega_chain=0), as for the finite differences.
 
-    python tests/golden/make_adjoint_tangent.py      # writes adjoint_tangent_<case>.npz
+    python tests/golden/make_adjoint_tangent.py         # writes adjoint_tangent_<case>.npz
+    python tests/golden/make_adjoint_tangent.py --full  # adjoint_tangent_full.npz
+
+--full: the adjoint workload itself (400 x 1200, one Bingham disk D=24,
+Bn=5, 4000 steps, J = mean v_y over steps 3000..4000), one process per
+gradient entry (about 14 minutes on 8 cores).
 """
 
 from __future__ import annotations
 
+import argparse
 import importlib
+import multiprocessing as mp
 import os
 import sys
 import time
@@ -53,7 +60,32 @@ def gradient(p, pin, n0: int, n1: int) -> tuple[float, np.ndarray]:
     return out[0][0], np.array([g for _, g in out])
 
 
+def _full_entry(args):
+    which, disk = args
+    cases = importlib.import_module("2d_nnf_lbm_b200").cases
+    p, pin, info = cases.workload_cfg5(0)
+    return tangent_j(p, pin, info["n0"], info["n1"], which, disk)
+
+
+def full() -> None:
+    ents = ac.parameters(1)
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(len(ents)) as pool:
+        out = pool.map(_full_entry, ents)
+    j, g = out[0][0], np.array([v for _, v in out])
+    np.savez(os.path.join(HERE, "adjoint_tangent_full.npz"), j=j, grad=g,
+             names=np.array([f"{e}{'' if q < 0 else q}" for e, q in ents]))
+    print(f"full: J={j:.10e} {time.time() - t0:.0f}s")
+    for (e, q), v in zip(ents, g):
+        print(f"   {e}{'' if q < 0 else q:<3} {v: .12e}")
+
+
 def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--full", action="store_true")
+    if ap.parse_args().full:
+        full()
+        return
     cases = importlib.import_module("2d_nnf_lbm_b200").cases
     for name in ac.CASES:
         t0 = time.time()

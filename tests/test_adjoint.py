@@ -315,3 +315,23 @@ def test_full_size_adjoint_against_gpu_fp64_differences(pkg, cases):
             allow = rtol * abs(fdh) + abs(fd - fdh)
             assert abs(g - fdh) <= allow, (name, g, fdh, allow)
     assert abs(j32 - j64) <= 1e-3 * abs(j64)
+
+
+@pytest.mark.gpu
+def test_full_size_adjoint_against_tangent_oracle(pkg, cases):
+    """The adjoint workload at its full size (400 x 1200, 4000 steps,
+    sqrt(N) checkpoints) against the forward-mode derivatives of the oracle
+    on the same inputs (tests/golden/adjoint_tangent_full.npz, made by
+    make_adjoint_tangent.py --full): FP64 within 1e-9, FP32 within 1e-4, of
+    each entry (plus that fraction of the position scale on the position
+    entries, x0 vanishing by symmetry)."""
+    t = np.load(os.path.join(GOLD, "adjoint_tangent_full.npz"))
+    names = list(map(str, t["names"]))
+    p64, pin, info = cases.workload_cfg5(0)
+    ps = position_scale(names, t["grad"])
+    for precision, rtol, jtol in ((0, 1e-9, 1e-10), (1, 1e-4, 1e-5)):
+        j, g, _ = adjoint_run(pkg, p64, pin, info["n0"], info["n1"], precision)
+        assert abs(j - float(t["j"])) <= jtol * abs(float(t["j"])), (precision, j)
+        for k, nm in enumerate(names):
+            allow = rtol * abs(t["grad"][k]) + (rtol * ps if nm.startswith(("x0", "y0")) else 0.0)
+            assert abs(g[k] - t["grad"][k]) <= allow, (precision, nm, g[k], t["grad"][k], allow)
