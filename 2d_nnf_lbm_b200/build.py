@@ -19,6 +19,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liblbm2d.so")
 BUILD_DIR = os.path.join(HERE, "_build")
+# the checked build: every computed index of the step, particle and batch
+# kernels checked against its buffer (LBM_CHECKED, lbm_checked_build() == 1)
+CHECKED_OUT = os.path.join(HERE, "liblbm2d_checked.so")
+CHECKED_BUILD_DIR = os.path.join(HERE, "_build_checked")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
@@ -49,7 +53,7 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 
 def build(verbose: bool = False, force: bool = False, out: str = OUT,
-          build_dir: str = BUILD_DIR, defines: tuple = ()) -> str:
+          build_dir: str = BUILD_DIR, defines: tuple = (), driver: bool = True) -> str:
     """Compile and link; ``defines`` (e.g. ("LBM_MINB_F32=6",)) tune launch
     bounds, ``out``/``build_dir`` place a variant elsewhere."""
     os.makedirs(build_dir, exist_ok=True)
@@ -78,7 +82,7 @@ def build(verbose: bool = False, force: bool = False, out: str = OUT,
     # the C++ driver that mirrors the reference's MAIN on the C ABI
     drv_src = os.path.join(HERE, "driver", "lbm_main.cpp")
     drv = os.path.join(os.path.dirname(out), "lbm_main")
-    if os.path.exists(drv_src) and (force or _stale(drv, [drv_src, out, *headers])):
+    if driver and os.path.exists(drv_src) and (force or _stale(drv, [drv_src, out, *headers])):
         cxx = shutil.which("g++") or "g++"
         cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"),
                drv_src, "-L", os.path.dirname(out), "-l:" + os.path.basename(out),
@@ -92,6 +96,11 @@ def build(verbose: bool = False, force: bool = False, out: str = OUT,
     if verbose:
         print("".join(logs))
     return out
+
+
+def build_checked(verbose: bool = False, force: bool = False) -> str:
+    """liblbm2d_checked.so beside liblbm2d.so (no driver of its own)."""
+    return build(verbose, force, CHECKED_OUT, CHECKED_BUILD_DIR, ("LBM_CHECKED",), driver=False)
 
 
 if __name__ == "__main__":

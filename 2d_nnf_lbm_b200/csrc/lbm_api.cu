@@ -182,6 +182,7 @@ int sticky_status(const lbm_sim* h) {
   if (s & ST_NAN) return LBM_E_NAN;
   if (s & ST_OVERFLOW) return LBM_E_OVERFLOW;
   if (s & ST_TIMEOUT) return LBM_E_TIMEOUT;
+  if (s & ST_BOUNDS) return LBM_E_BOUNDS;
   if (s & ST_PARTICLE) return LBM_E_PARTICLE;
   return LBM_OK;
 }
@@ -1466,6 +1467,14 @@ int lbm_selftest_wait(lbm_sim* h, int32_t limit) {
   return LBM_OK;
 }
 
+int32_t lbm_checked_build(void) {
+#ifdef LBM_CHECKED
+  return 1;
+#else
+  return 0;
+#endif
+}
+
 const char* lbm_strerror(int code) {
   switch (code) {
     case LBM_OK: return "ok";
@@ -1482,6 +1491,7 @@ const char* lbm_strerror(int code) {
     case LBM_E_PARTICLE: return "particle outside the lattice";
     case LBM_E_ABI: return "lbm_params.struct_size mismatch";
     case LBM_E_SCRATCH: return "lattice or particle count exceeds the fixed no-alloc scratch";
+    case LBM_E_BOUNDS: return "a kernel index check failed (checked build)";
     default: return "unknown error";
   }
 }

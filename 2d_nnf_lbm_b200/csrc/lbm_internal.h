@@ -68,7 +68,24 @@ enum : int {
   ST_OVERFLOW = 2,
   ST_TIMEOUT = 4,
   ST_PARTICLE = 8,
+  ST_BOUNDS = 16,  // checked build: an index check failed, the access was skipped
 };
+
+// Index checks of the checked build (compiled with LBM_CHECKED): an index
+// outside [0, n) of its buffer sets ST_BOUNDS in the handle's status word and
+// the guarded access is skipped, so a wrong index shows as LBM_E_BOUNDS
+// instead of reading or writing memory it should not.  The ordinary build
+// compiles every check to true.
+#ifdef LBM_CHECKED
+__device__ __forceinline__ bool lbm_in_range(long long i, long long n, int* status) {
+  if (i >= 0 && i < n) return true;
+  atomicOr(status, ST_BOUNDS);
+  return false;
+}
+#define LBM_IN(i, n, st) lbm_in_range((long long)(i), (long long)(n), (st))
+#else
+#define LBM_IN(i, n, st) true
+#endif
 
 struct Geometry {
   int nx, ny;        // cells; nodes 0..nx, 0..ny

@@ -1127,6 +1127,7 @@ struct CandList {
 __device__ __forceinline__ CandList cand_list(const LatticeArgs& a, int lt, int buf, int lane) {
   CandList c{0, 0};
   if (buf < 0) return c;  // a tile that no disk can reach
+  if (!LBM_IN(lt, a.ntiles, a.status)) return c;
   const long long tbase = (long long)buf * a.ntiles + lt;
   c.n = a.tile_count[tbase];
   if (lane < a.tile_cap) c.idx = a.tile_list[tbase * a.tile_cap + lane];
@@ -1148,14 +1149,16 @@ __device__ __forceinline__ void cand_copy(const LatticeArgs& a, CandList c, int 
   }
   if (lane < c.n) {
     C.idx[lane] = c.idx;
-    const double* p = a.ps + c.idx;
-    const long long st = a.npad;
-    cp_async8(&C.px[lane], p + P_X * st);
-    cp_async8(&C.py[lane], p + P_Y * st);
-    cp_async8(&C.pd[lane], p + P_D * st);
-    cp_async8(&C.pu[lane], p + P_U * st);
-    cp_async8(&C.pv[lane], p + P_V * st);
-    cp_async8(&C.pw[lane], p + P_W * st);
+    if (LBM_IN(c.idx, a.np, a.status)) {
+      const double* p = a.ps + c.idx;
+      const long long st = a.npad;
+      cp_async8(&C.px[lane], p + P_X * st);
+      cp_async8(&C.py[lane], p + P_Y * st);
+      cp_async8(&C.pd[lane], p + P_D * st);
+      cp_async8(&C.pu[lane], p + P_U * st);
+      cp_async8(&C.pv[lane], p + P_V * st);
+      cp_async8(&C.pw[lane], p + P_W * st);
+    }
   }
   // the barrier's phase waits for this lane's copies (pending count +1 now,
   // -1 when they land); c.n is warp-uniform
@@ -1316,7 +1319,7 @@ __device__ __forceinline__ void node_gather(const LatticeArgs& a, const StepIO<T
         waited = true;
       }
       const int comp = lane >> 3;
-      if ((lane & 7) == 0 && comp < 3) {
+      if ((lane & 7) == 0 && comp < 3 && LBM_IN(C.idx[c], a.np, a.status)) {
         const long long st = a.npad;
         unsigned long long* acc = a.facc + C.idx[c] + 2 * comp * st;
         facc_add(acc, acc + st, tot);
@@ -1345,6 +1348,7 @@ __device__ __forceinline__ void node_collide(const LatticeArgs& a, const StepIO<
   constexpr bool F64 = sizeof(T) == 8;
   const Model& m = a.m;
   const long long P = a.g.plane;
+  if (!LBM_IN(nd, P, a.status)) return;  // every store below is at offset nd of a plane
   T* __restrict__ dst = io.dst;
   // ---- velocity correction (C1:1138-1152) and collision of the next step
   const T uxc = v.ux + (T)0.5 * (v.gx + (T)0.0);

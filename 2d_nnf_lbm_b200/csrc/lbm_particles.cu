@@ -92,8 +92,11 @@ __device__ __forceinline__ void insert_tiles(const ParticleArgs& a, int p, doubl
       tt[u] = -1;
       if (t < nt) {
         const int ty = t / ntx, tx = t - ty * ntx;
-        tt[u] = (ty0 + ty) * a.nbx + tx0 + tx;
-        sl[u] = atomicAdd(&cnt[tt[u]], 1);
+        const int tile = (ty0 + ty) * a.nbx + tx0 + tx;
+        if (LBM_IN(tile, a.ntiles, a.status)) {
+          tt[u] = tile;
+          sl[u] = atomicAdd(&cnt[tile], 1);
+        }
       }
     }
 #pragma unroll
@@ -150,12 +153,16 @@ __device__ void build_tile_order(const ParticleArgs& a, int buf) {
     const int ex = before + inc - v;
     if (un) {
       const int pos = s_base[0] + (ex & 0xffff);
-      ord[pos] = t;
-      rev[total_u - 1 - pos] = t;
+      if (LBM_IN(pos, total_u, a.status)) {
+        ord[pos] = t;
+        rev[total_u - 1 - pos] = t;
+      }
     } else if (in) {
       const int pos = total_u + s_base[1] + (ex >> 16);
-      ord[pos] = t;
-      rev[a.ntiles - 1 + total_u - pos] = t;
+      if (LBM_IN(pos, a.ntiles, a.status) && LBM_IN(pos - total_u, a.ntiles - total_u, a.status)) {
+        ord[pos] = t;
+        rev[a.ntiles - 1 + total_u - pos] = t;
+      }
     }
     __syncthreads();
     if (tid == 0) {
@@ -224,7 +231,7 @@ __device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
   __syncthreads();
   for (int p = tid; p < a.np; p += PBLK) {
     const int slot = atomicAdd(&S.cnt[S.key[p] & (HASH - 1)], 1);
-    S.items[slot] = p;
+    if (LBM_IN(slot, a.np, a.status)) S.items[slot] = p;
   }
   __syncthreads();
   for (int p = tid; p < a.np; p += PBLK) {
@@ -239,7 +246,7 @@ __device__ void rebuild_pairs(const ParticleArgs& a, PShared& S) {
         const int b = ck & (HASH - 1);
         for (int s = S.start[b]; s < S.start[b + 1]; ++s) {
           const int q = S.items[s];
-          if (q == p || S.key[q] != ck) continue;
+          if (!LBM_IN(q, a.np, a.status) || q == p || S.key[q] != ck) continue;
           const double dx = px - S.x[q], dy = py - S.y[q];
           const double lim = 0.5 * pd + 0.5 * S.d[q] + a.rep_zeta + SKIN;
           if (dx * dx + dy * dy > lim * lim) continue;
@@ -354,12 +361,14 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
     const double px = S.x[p], py = S.y[p], pd = S.d[p];
     double fcx = 0.0, fcy = 0.0;
     if (a.np > 1) {
-      const int nn = a.nbr_count[p];
+      int nn = a.nbr_count[p];
+      if (!LBM_IN(nn, MAX_NEIGH + 1, a.status)) nn = 0;
       int nbl[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) nbl[k] = k < nn ? a.nbr[(long long)k * a.npad + p] : 0;
       for (int k = 0; k < nn; ++k) {
         const int q = k < 8 ? nbl[k] : a.nbr[(long long)k * a.npad + p];
+        if (!LBM_IN(q, a.np, a.status)) continue;
         double F[2];
         if (q < p) {
           pair_force(a, S.x[q], S.y[q], S.d[q], px, py, pd, stale, F);

@@ -33,6 +33,8 @@ ERRORS = {
     -8: "LBM_E_STATE",
     -9: "LBM_E_PARTICLE",
     -10: "LBM_E_ABI",
+    -11: "LBM_E_SCRATCH",
+    -12: "LBM_E_BOUNDS",
 }
 LBM_FP64, LBM_FP32_SHIFTED = 0, 1
 LBM_BC_ZOUHE, LBM_BC_HALFWAY_BB, LBM_BC_EQUILIBRIUM = 0, 1, 2
@@ -226,7 +228,9 @@ class LbmError(RuntimeError):
 
 
 def library_path() -> str:
-    return os.path.join(_HERE, "liblbm2d.so")
+    """liblbm2d.so of the package directory, or the library LBM2D_LIBRARY
+    names (e.g. the checked build, liblbm2d_checked.so)."""
+    return os.environ.get("LBM2D_LIBRARY") or os.path.join(_HERE, "liblbm2d.so")
 
 
 _LIB = None
@@ -270,6 +274,7 @@ def load_library():
         "lbm_profile": ([vp, ctypes.c_int32], ctypes.c_int),
         "lbm_profile_read": ([vp, dp, P(ctypes.c_int64)], ctypes.c_int),
         "lbm_strerror": ([ctypes.c_int], ctypes.c_char_p),
+        "lbm_checked_build": ([], ctypes.c_int32),
         "lbm_fields_noalloc": ([P(LbmParams), vp, ctypes.c_int32, vp, vp, vp], ctypes.c_int),
         "lbm_adjoint": ([vp, P(LbmObjective), dp, dp], ctypes.c_int),
         "lbm_batch_create": ([P(LbmParams), ctypes.c_int32, P(vp)], ctypes.c_int),

@@ -47,7 +47,9 @@ enum {
     LBM_E_PARTICLE = -9,  /* particle outside the lattice, or input disks that
                              overlap (lbm_set_particles)                      */
     LBM_E_ABI = -10,      /* struct_size does not match this library          */
-    LBM_E_SCRATCH = -11   /* input larger than lbm_fields_noalloc's scratch   */
+    LBM_E_SCRATCH = -11,  /* input larger than lbm_fields_noalloc's scratch   */
+    LBM_E_BOUNDS = -12    /* checked build only: a kernel's index check failed
+                             and the access was skipped                       */
 };
 
 /* ---- variant switches (compile-time PARAMETERs / IF(0|1) blocks upstream) */
@@ -277,6 +279,13 @@ int lbm_profile(lbm_sim* h, int32_t enable);
 int lbm_profile_read(lbm_sim* h, double* ms, int64_t* launches);
 
 const char* lbm_strerror(int code);
+
+/* 1 in the checked build of this library (liblbm2d_checked.so: every
+ * computed index of the step, particle and batch kernels is checked against
+ * its buffer; a failed check skips the access and reports LBM_E_BOUNDS), 0
+ * in the ordinary build.  The reference has no counterpart: its Fortran is
+ * built without array bounds checks. */
+int32_t lbm_checked_build(void);
 
 /* Adjoint gradients of a particle observable (no counterpart in the
  * reference, which has no derivatives).  The objective is the mean of one
