@@ -23,7 +23,7 @@
 
 namespace lbm {
 
-constexpr int PBLK = 1024;
+constexpr int PBLK = 512;
 constexpr int HASH = 4096;  // power of two
 
 struct PShared {
@@ -359,33 +359,24 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
     const double rhop = P[P_RHO], M = P[P_M], I = P[P_I], ang = P[P_ANG];
     const double xt = P[P_XT], yt = P[P_YT];
     const double px = S.x[p], py = S.y[p], pd = S.d[p];
-    double fcx = 0.0, fcy = 0.0;
+    // The neighbour count and the first 8 list entries load together (the
+    // list has room for MAX_NEIGH entries of every disk; those past the
+    // count are masked below), and the wall forces, which need neither, are
+    // formed while they are in flight.  The sums keep the order of the
+    // reference: the pairs, then walls 1 to 4.
+    int nn = 0, nraw[8];
     if (a.np > 1) {
-      int nn = a.nbr_count[p];
-      if (!LBM_IN(nn, MAX_NEIGH + 1, a.status)) nn = 0;
-      int nbl[8];
+      nn = a.nbr_count[p];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) nbl[k] = k < nn ? a.nbr[(long long)k * a.npad + p] : 0;
-      for (int k = 0; k < nn; ++k) {
-        const int q = k < 8 ? nbl[k] : a.nbr[(long long)k * a.npad + p];
-        if (!LBM_IN(q, a.np, a.status)) continue;
-        double F[2];
-        if (q < p) {
-          pair_force(a, S.x[q], S.y[q], S.d[q], px, py, pd, stale, F);
-          fcx = fcx - F[0];
-          fcy = fcy - F[1];
-        } else {
-          pair_force(a, px, py, pd, S.x[q], S.y[q], S.d[q], stale, F);
-          fcx = fcx + F[0];
-          fcy = fcy + F[1];
-        }
-      }
+      for (int k = 0; k < 8; ++k) nraw[k] = a.nbr[(long long)k * a.npad + p];
     }
+    double wf0[4] = {0.0, 0.0, 0.0, 0.0}, wf1[4] = {0.0, 0.0, 0.0, 0.0};
     // walls (C1:735-768 mirror images; C3:775-804 wall disks)
     if (a.wall_model != 2) {
       const double ZITA = a.rep_zeta, CIJ = a.c_ij, EPS_W = a.eps_w, E_W = a.e_w;
       const double x = px, y = py, D = pd;
       double D_PW = stale;
+#pragma unroll
       for (int iw = 1; iw <= 4; ++iw) {
         double rw0, rw1;
         if (a.wall_model == 0) {
@@ -413,10 +404,38 @@ __device__ __forceinline__ void particles_body(const ParticleArgs& a) {
             F1 = (EPS_W * CIJ * (q * q) + e) * ey / D_PW;
           }
         }
-        fcx = fcx + F0;
-        fcy = fcy + F1;
+        wf0[iw - 1] = F0;
+        wf1[iw - 1] = F1;
       }
       if (p == a.np - 1) *a.stale_dpw = D_PW;
+    }
+    double fcx = 0.0, fcy = 0.0;
+    if (a.np > 1) {
+      if (!LBM_IN(nn, MAX_NEIGH + 1, a.status)) nn = 0;
+      int nbl[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) nbl[k] = k < nn ? nraw[k] : 0;
+      for (int k = 0; k < nn; ++k) {
+        const int q = k < 8 ? nbl[k] : a.nbr[(long long)k * a.npad + p];
+        if (!LBM_IN(q, a.np, a.status)) continue;
+        double F[2];
+        if (q < p) {
+          pair_force(a, S.x[q], S.y[q], S.d[q], px, py, pd, stale, F);
+          fcx = fcx - F[0];
+          fcy = fcy - F[1];
+        } else {
+          pair_force(a, px, py, pd, S.x[q], S.y[q], S.d[q], stale, F);
+          fcx = fcx + F[0];
+          fcy = fcy + F[1];
+        }
+      }
+    }
+    if (a.wall_model != 2) {
+#pragma unroll
+      for (int iw = 0; iw < 4; ++iw) {
+        fcx = fcx + wf0[iw];
+        fcy = fcy + wf1[iw];
+      }
     }
     P[P_FCX] = fcx;
     P[P_FCY] = fcy;
