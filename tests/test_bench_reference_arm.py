@@ -33,6 +33,7 @@ def test_reference_arm_prints_one_contract_line():
     assert d["value"] > 0.0
     assert (d["n_gpus"], d["steps"], d["warmup"]) == (1, 3, 3)
     assert d["config"]["nodes"] == 65 * 129 and d["config"]["particles"] == 4
+    assert "smaller than L2" in d["config"]["l2"]
     base = d["cpu_baseline"]
     assert base["kind"] == "port" and base["cores"] == 1
     assert base["value"] == d["value"] and base["unit"] == "MLUPS"
@@ -45,3 +46,11 @@ def test_reference_arm_other_ranks_exit_without_output():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+def test_l2_note_of_the_bench_workload():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.l2_note(1025 * 2049) == (
+        "working set per step 151 MB (fp32) / 302 MB (fp64) > 126 MB L2; no flush")
