@@ -758,7 +758,7 @@ def main():
         "l2": l2_note(nodes),
         "parallelism": f"replicas x{world}",
     }
-    metric = "MLUPS (FP32-shifted, multi-particle 1024x2048, 512 disks)"
+    metric = f"MLUPS (FP32-shifted, multi-particle {args.nx}x{args.ny}, {args.particles} disks)"
 
     if args.impl == "reference":
         if rank != 0:

@@ -28,7 +28,7 @@ def test_reference_arm_prints_one_contract_line():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference"
-    assert d["metric"].startswith("MLUPS")
+    assert d["metric"] == "MLUPS (FP32-shifted, multi-particle 64x128, 4 disks)"
     assert d["unit"] == "MLUPS" and d["higher_is_better"] is True
     assert d["value"] > 0.0
     assert (d["n_gpus"], d["steps"], d["warmup"]) == (1, 3, 3)
