@@ -7,7 +7,8 @@ state they reach as .npz files beside this script:
     python tests/golden/make_golden.py [--reference PATH]
 
 Cases (every run is the unmodified main program and subroutines of the file
-named; only PARAMETERs and the particle input file are replaced):
+named; only PARAMETERs and the particle input file are replaced, and in the
+c1_bgk cases the collision call of the main program, as described there):
 
   c1_center  1_Disk_Newtonian (C1), NX=24 NY=40, one disk D=8 rho_p=1.25 at
              (12, 28), 40 steps: Zou-He walls, MRT, SPM coupling, Newton-Euler
@@ -23,6 +24,15 @@ named; only PARAMETERs and the particle input file are replaced):
              (NON_NEWTONIAN=.TRUE.): Papanastasiou viscosity with the strain
              rate of C1:896-948 (m_neq against COMPUTEFEQNEW's moments) and
              the node-to-node omega chain
+  c1_bgk     C1 as c1_center with its main program calling COLLISION
+             (C1:774-841, the single-relaxation BGK routine) in place of
+             Collision_MRT: the call the program carries commented out at
+             C1:295 is switched in and the Collision_MRT call of C1:296 is
+             skipped; nothing else changes
+  c1_bgk_biviscous  c1_bgk with NON_NEWTONIAN=.TRUE. and TAU_Y=1.0D-5:
+             COLLISION's bi-viscosity branch (GAMMA_C = TAU_Y/(MU_R - MU_0),
+             MU_R = 1000 MU_0), about a third of the nodes unyielded at the
+             last step
   c1_error   C1 at NX=16 NY=24 with the disk at (8, 14), D=6, 2000 steps:
              the reference's COMPUTEERROR values at steps 1000 and 2000 (unit 7)
   c3_casson  C3 as c3_multi with its non-Newtonian branch switched on
@@ -73,6 +83,16 @@ CASES = {
     "c1_nonnewt": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
                        overrides={"NX": "24", "NY": "40", "TIME_MAX": "40", "NON_NEWTONIAN": ".TRUE."},
                        particles="12\t28\t8\t1.25", steps=40),
+    "c1_bgk": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
+                   overrides={"NX": "24", "NY": "40", "TIME_MAX": "40"},
+                   particles="12\t28\t8\t1.25", steps=40,
+                   edits={295: ("!CALL COLLISION(", "CALL COLLISION(")}, skip_lines=[296]),
+    "c1_bgk_biviscous": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
+                             overrides={"NX": "24", "NY": "40", "TIME_MAX": "40",
+                                        "NON_NEWTONIAN": ".TRUE.", "TAU_Y": "1.0D-5"},
+                             particles="12\t28\t8\t1.25", steps=40,
+                             edits={295: ("!CALL COLLISION(", "CALL COLLISION(")},
+                             skip_lines=[296]),
     "c1_error": dict(file="1_Disk_Newtonian/D2Q9_1P_Validated_20190530.f90",
                      overrides={"NX": "16", "NY": "24", "TIME_MAX": "2000"},
                      particles="8\t14\t6\t1.25", steps=2000),
@@ -101,6 +121,12 @@ PARTICLE_FIELDS = ["CENTER", "VELOCITY", "FORCE", "F_COL", "DIAM", "RHO_P", "M_P
 
 def run_case(ref_root, name, spec):
     src = open(os.path.join(ref_root, spec["file"]), encoding="latin-1").read()
+    lines = src.split("\n")
+    for ln, (old, new) in spec.get("edits", {}).items():  # 1-based line numbers
+        if old not in lines[ln - 1]:
+            raise SystemExit(f"{name}: line {ln} does not hold {old!r}")
+        lines[ln - 1] = lines[ln - 1].replace(old, new, 1)
+    src = "\n".join(lines)
     files = {"0_Particle_Initial_Position.txt": spec["particles"]} if spec["particles"] else {}
     t0 = time.time()
     frame, io, prog = f90run.run_program(src, overrides=spec["overrides"], files=files, stubs=STUBS,

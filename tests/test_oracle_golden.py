@@ -42,6 +42,15 @@ def _setup(cases, name):
         p.rheology = 1        # LBM_BINGHAM (Papanastasiou, C1:950-954)
         p.strain_model = 1    # LBM_STRAIN_FEQ (C1:896-948)
         return p, cases.pin_array([[12.0, 28.0]], 8.0, 1.25), {"omega_chain": 1}
+    if name in ("c1_bgk", "c1_bgk_biviscous"):
+        # C1's main program calling COLLISION (C1:774-841) in place of
+        # Collision_MRT; the bi-viscous run at TAU_Y = 1.0D-5
+        p = cases.shipped_c1(24, 40, 8.0)
+        p.collision = 1  # LBM_COLLISION_BGK
+        if name == "c1_bgk_biviscous":
+            p.rheology = 1  # LBM_BINGHAM: COLLISION's bi-viscosity branch
+            p.tau_y = 1.0e-5
+        return p, cases.pin_array([[12.0, 28.0]], 8.0, 1.25), {}
     if name == "c3_casson":
         p = cases.shipped_c3(48, 72)
         p.rheology = 2  # LBM_CASSON
@@ -59,7 +68,8 @@ def _setup(cases, name):
     raise KeyError(name)
 
 
-CASES = ["c1_center", "c1_walls", "c1_nonnewt", "c6_bingham", "c3_multi", "c3_casson", "c2_dkt", "c4_oscillate"]
+CASES = ["c1_center", "c1_walls", "c1_nonnewt", "c1_bgk", "c1_bgk_biviscous", "c6_bingham",
+         "c3_multi", "c3_casson", "c2_dkt", "c4_oscillate"]
 
 
 def _exact(a, b, what):
@@ -127,6 +137,11 @@ def test_goldens_cover_the_branches_they_claim():
     om = c6["OMEGA_BN"]
     assert om.min() < om.max()                                # Bingham omega varies
     assert np.any(c6["DISK_ANGLE"] != 0) or np.any(c6["DISK_VELOCITY"][:, 2] != 0)
+    # the BGK runs took COLLISION, not Collision_MRT, and the bi-viscous one
+    # has yielded and unyielded nodes (omega = 1/(3 MU_R + 1/2) when unyielded)
+    assert not np.array_equal(_load("c1_bgk")["F"], _load("c1_center")["F"])
+    bv = _load("c1_bgk_biviscous")["OMEGA_BN"]
+    assert 0 < np.count_nonzero(bv < 0.01) < bv.size
 
 
 def test_oracle_compute_error_matches_reference(cases):
